@@ -1,0 +1,167 @@
+/*
+ * aero3d.h - C ABI of the B200 3D Euler cut-cell solver (libaero3d.so).
+ *
+ * Drop-in for the solver entry points of WeiJungSong/3d_aero_lab `src/air_cfd.js`:
+ * grid generation, cut-cell geometry (volume fractions, face apertures, thin-wing
+ * baffles, fixed-state engine cells), the SSP-RK2 solver object and the force,
+ * Trefftz and residual post-processing.  The reference calls these from JavaScript;
+ * a Node N-API shim binds these functions one to one.
+ *
+ * Conventions
+ *  - Every function returns an int status (A3D_OK == 0).  No exception crosses the
+ *    ABI and there is no CPU fallback: if the GPU is missing or a CUDA call fails the
+ *    status says so and a3d_last_error() returns the message of the failing call.
+ *  - Only plain C types cross the ABI: pointers, sizes, doubles, floats.
+ *  - Cell index q = (k*NY + j)*NX + i (src/air_cfd.js:45).
+ *  - Conservative state is structure-of-arrays float32 (rho, rho*u, rho*v, rho*w, E),
+ *    nondimensional with rho_inf = 1, a_inf = 1, p_inf = 1/gamma (src/air_cfd.js:8).
+ *  - Solver calls are asynchronous on the solver's own CUDA stream except the ones
+ *    that return host data (read, forces, trefftz, residual, diag), which synchronise.
+ */
+#ifndef AERO3D_H
+#define AERO3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---------------------------------------------------------------- */
+#define A3D_OK             0
+#define A3D_ERR_ARG        1  /* bad argument (null pointer, size out of range)          */
+#define A3D_ERR_CUDA       2  /* a CUDA runtime call failed; see a3d_last_error()         */
+#define A3D_ERR_NOMEM      3  /* device allocation failed                                 */
+#define A3D_ERR_NONFINITE  4  /* the state holds NaN or Inf (detected on the device)      */
+#define A3D_ERR_STATE      5  /* call not valid in the object's current state            */
+#define A3D_ERR_BUDGET     6  /* request does not fit the server's device-memory budget  */
+#define A3D_ERR_TIMEOUT    7  /* a bounded wait ran out                                   */
+#define A3D_ERR_NODEVICE   8  /* no CUDA device is visible                                */
+
+#define A3D_MAX_ENGINES 2
+#define A3D_MAX_EXITS   2
+#define A3D_ENV_N       300   /* nacelle envelope table intervals (src/air_cfd.js:53)   */
+
+/* ---- aircraft shape: what the inside tests need (src/aircraft.js, src/air_field.js) -- */
+typedef struct a3d_surface {
+  double x0, z0, semi, cr, ct;   /* root LE x, root z, semi-span (height for the fin), chords */
+  double tanL;                   /* tan(sweep) as makeSurface computes it (aircraft.js:83)   */
+  double tanD_pt, tanI_pt;       /* tan(dihedral), tan(incidence) used by surface points     */
+  double tanD_deg, tanI_deg;     /* the same via DEG, as inLift/zMean compute them           */
+  double tcR, tcT, camber;       /* thickness ratios root/tip, NACA camber                   */
+  double sA;                     /* AirGeom attachment span (air_field.js:107)              */
+  double bb[4];                  /* AirGeom bounding box x0, x1, z0, z1 (air_field.js:109)  */
+} a3d_surface;
+
+typedef struct a3d_engine {
+  double x0, y, z;               /* lip station and axis (aircraft.js:132-141)               */
+  int32_t internal;              /* 1: engine buried in the fuselage                          */
+  int32_t env_n;                 /* 0: no nacelle envelope, else A3D_ENV_N                    */
+  double env_xmax;               /* envelope length                                          */
+  float env_R[A3D_ENV_N + 1];    /* envelope radius table, float32 (air_cfd.js:53-54)       */
+  float pad_;
+} a3d_engine;
+
+typedef struct a3d_exit {
+  int32_t type;                  /* fixed-state cell type: 4 bypass jet, 5 core jet          */
+  int32_t pad_;
+  double x, R, Rin;              /* exit station (engine frame), outer/inner radius          */
+} a3d_exit;
+
+typedef struct a3d_shape {
+  double fus_L, fus_R0, fus_Ln, fus_Lt, fus_xt0, fus_Re, fus_noseP, fus_tailUp;
+  a3d_surface wing, htail, vtail;
+  double ref_b;                  /* reference span (cfdGrid core width)                      */
+  double view_Rmax;              /* engine outer radius (cfdGrid margins)                    */
+  double lip_x, lip_r;           /* intake lip (inlet sink layer)                            */
+  int32_t n_engines, n_exits;
+  a3d_engine engines[A3D_MAX_ENGINES];
+  a3d_exit exits[A3D_MAX_EXITS];
+} a3d_shape;
+
+/* ---- library ------------------------------------------------------------------------ */
+/* Message of the last failure on this thread ("" if none). */
+const char* a3d_last_error(void);
+/* ABI version, bumped on any change of a struct or signature. */
+int a3d_abi_version(void);
+
+/* ---- grid: cfdAxis/cfdGrid (src/air_cfd.js:14-44) -------------------------------- */
+/* Builds the stretched half-domain grid for `target_cells`.  Face coordinates go to
+ * xf/yf/zf (capacity `cap` each, float64, NX+1 / NY+1 / NZ+1 values); dims gets
+ * NX, NY, NZ; h_out the near-body spacing; core_out the core box x0,x1,y1,z0,z1.   */
+int a3d_grid_build(const a3d_shape* shape, double target_cells, int32_t cap,
+                   double* xf, double* yf, double* zf, int32_t dims[3],
+                   double* h_out, double core_out[5]);
+
+/* ---- cut-cell geometry: cfdGeom (src/air_cfd.js:50-141), on the GPU ---------------- */
+/* Evaluates the inside tests on the device and returns the reference's arrays:
+ * t (u8[N]: 0 fluid, 1 solid, 3 inlet sink, 4 bypass jet, 5 core jet), phi (f32[N]),
+ * ap0..ap2 (f32[N], +x/+y/+z face apertures), ap3 (f32[N], baffle slope dz/dx on
+ * the +z face).  counts gets nSolid, nCut; vol gets volW, volH, volV.
+ * Any of the output pointers may be NULL to skip that copy.                          */
+int a3d_geom_build(const a3d_shape* shape, const int32_t dims[3],
+                   const double* xf, const double* yf, const double* zf,
+                   double h, double delta_deg,
+                   uint8_t* t, float* phi, float* ap0, float* ap1, float* ap2, float* ap3,
+                   int64_t counts[2], int32_t vol[3]);
+
+/* ---- force list: cfdForceList (src/air_cfd.js:143-152), on the GPU ----------------- */
+/* Number of list cells; then the list itself in cell order (any pointer may be NULL). */
+typedef struct a3d_solver a3d_solver;
+int a3d_solver_force_list(a3d_solver* s, int64_t* n_out, int64_t cap,
+                          int64_t* q, double* cx, double* cz, double* x, double* z);
+
+/* ---- solver object: CfdCPU/CfdGPU (src/air_cfd.js:157-259, 367-438) -------------- */
+/* From caller geometry arrays, like `new CfdGPU(g, geo)`.  The arrays are copied to the
+ * device; the caller keeps ownership.                                                 */
+int a3d_solver_create(const int32_t dims[3], const double* xf, const double* yf,
+                      const double* zf, const uint8_t* t, const float* phi,
+                      const float* ap0, const float* ap1, const float* ap2,
+                      const float* ap3, int device, a3d_solver** out);
+/* Builds grid-resident geometry straight on the device from the shape (no host copy of
+ * the N-sized arrays): cfdGeom + cfdForceList + solver in one call.                   */
+int a3d_solver_create_shape(const a3d_shape* shape, const int32_t dims[3],
+                            const double* xf, const double* yf, const double* zf,
+                            double h, double delta_deg, int device, a3d_solver** out);
+int a3d_solver_destroy(a3d_solver* s);
+/* Grid size and the device the solver lives on. */
+int a3d_solver_dims(a3d_solver* s, int32_t dims[3], int64_t* n_cells);
+/* opt.cfl and opt.order (defaults 0.7 and 2, src/air_cfd.js:162). */
+int a3d_solver_set_opt(a3d_solver* s, double cfl, int32_t order);
+/* setFree(F[5]) (src/air_cfd.js:166): far-field conservative state. */
+int a3d_solver_set_free(a3d_solver* s, const double F[5]);
+/* setFix([sink, jetBypass, jetCore]) (src/air_cfd.js:167): 3 x 5 conservative states
+ * for cell types 3, 4, 5.                                                             */
+int a3d_solver_set_fix(a3d_solver* s, const double fix[15]);
+/* reset() (src/air_cfd.js:168): Q = F everywhere, it = 0. */
+int a3d_solver_reset(a3d_solver* s);
+/* step(n) (src/air_cfd.js:252-258): n SSP-RK2 iterations, queued on the solver stream. */
+int a3d_solver_step(a3d_solver* s, int32_t n);
+/* Iterations done since reset. */
+int a3d_solver_iterations(a3d_solver* s, int64_t* it);
+/* read() (src/air_cfd.js:259): copies Q into five caller arrays of N floats
+ * (rho, rho*u, rho*v, rho*w, E).  Synchronises.                                        */
+int a3d_solver_read(a3d_solver* s, float* r, float* ru, float* rv, float* rw, float* E);
+/* Uploads a state (warm start or checkpoint restore); same layout as read(). */
+int a3d_solver_write(a3d_solver* s, const float* r, const float* ru, const float* rv,
+                     const float* rw, const float* E);
+/* cfdForces (src/air_cfd.js:443-452) over the force list, FP64 on the device.
+ * out = {CL, CD, Cm}.  M is used as given (the controller passes max(M, 0.05)).       */
+int a3d_solver_forces(a3d_solver* s, double alpha_deg, double M, double S, double xcg,
+                      double zcg, double cref, double out[3]);
+/* Trefftz-plane induced drag at station xT (src/air_cfd.js:560-570), FP64. */
+int a3d_solver_trefftz(a3d_solver* s, double xT, double alpha_deg, double M, double S,
+                       double* cdi);
+/* Density residual (src/air_cfd.js:552-555): RMS of rho - rho_prev over fluid cells with
+ * q % stride == 0, divided by the iterations since the previous call, in FP64; then
+ * rho_prev = rho.  The first call only takes the snapshot and returns -1.
+ * Returns A3D_ERR_NONFINITE if a sampled density is NaN/Inf.                          */
+int a3d_solver_residual(a3d_solver* s, int32_t stride, double* res);
+/* Largest Mach number over fluid cells with q % stride == 0 (src/air_cfd.js:571). */
+int a3d_solver_mach_max(a3d_solver* s, int32_t stride, double* mmax);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AERO3D_H */

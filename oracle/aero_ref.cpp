@@ -1,0 +1,698 @@
+/*
+ * aero_ref.cpp - CPU ORACLE (test infrastructure only, never shipped or measured as
+ * the product): a line-by-line restatement of the reference's 3D Euler cut-cell path
+ * in WeiJungSong/3d_aero_lab `src/air_cfd.js`.
+ *
+ *   grid      cfdAxis / cfdGrid          src/air_cfd.js:14-44
+ *   geometry  cfdGeom (+ AirGeom tests)  src/air_cfd.js:50-141, src/air_field.js:115-134
+ *   forces    cfdForceList / cfdForces   src/air_cfd.js:143-152, 443-452
+ *   solver    CfdCPU                     src/air_cfd.js:157-259
+ *   post      Trefftz, residual, Mmax    src/air_cfd.js:552-572
+ *
+ * Numerics follow the reference: float32 storage for the state, the grid centres
+ * and spacings, phi and apertures; float64 arithmetic everywhere (JavaScript numbers).
+ * A second solver instantiation keeps the state in float64 ("FP64 run of the same
+ * scheme").  Loops keep the reference's k, j, i order; OpenMP only splits loops whose
+ * iterations are independent, so every thread count gives bit-identical results.
+ *
+ * Only tests/, __graft_entry__.smoke() and bench.py's CPU baseline load this library.
+ */
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+#include "../include/aero3d.h"
+
+namespace {
+
+const double CG = 1.4;                       // src/air_cfd.js:11
+const double PI = 3.141592653589793;
+const double DEG = PI / 180;                 // src/field.js:7
+const double SUB[3] = {1.0 / 6, 0.5, 5.0 / 6};  // src/air_cfd.js:72
+
+double js_round(double x) {                  // Math.round: ties toward +infinity
+  double r = std::floor(x);
+  return (x - r >= 0.5) ? r + 1 : r;
+}
+
+/* ---------------- aircraft pieces needed by the inside tests ---------------- */
+double nacaT(double t, double x) {           // src/aircraft.js:58
+  x = std::max(0.0, std::min(1.0, x));
+  return 5 * t * (0.2969 * std::sqrt(x) - 0.126 * x - 0.3516 * x * x + 0.2843 * std::pow(x, 3) - 0.1036 * std::pow(x, 4));
+}
+double nacaC(double m, double x) {           // src/aircraft.js:59 (p = 0.4)
+  const double p = 0.4;
+  if (m == 0) return 0;
+  return x < p ? m / (p * p) * (2 * p * x - x * x) : m / std::pow(1 - p, 2) * ((1 - 2 * p) + 2 * p * x - x * x);
+}
+double surf_chord(const a3d_surface& S, double s) { return S.cr + (S.ct - S.cr) * s / S.semi; }
+double surf_xLE(const a3d_surface& S, double s) { return S.x0 + s * S.tanL; }
+double surf_tc(const a3d_surface& S, double s) { return S.tcR + (S.tcT - S.tcR) * s / S.semi; }
+
+double fus_R(const a3d_shape& a, double x) { // src/aircraft.js:66-72
+  if (x <= 0) return 0;
+  if (x < a.fus_Ln) { double s = 1 - x / a.fus_Ln; return a.fus_R0 * std::pow(std::max(0.0, 1 - s * s), a.fus_noseP); }
+  if (x <= a.fus_xt0) return a.fus_R0;
+  if (x >= a.fus_L) return a.fus_Re;
+  double t = (x - a.fus_xt0) / a.fus_Lt;
+  return a.fus_Re + (a.fus_R0 - a.fus_Re) * 0.5 * (1 + std::cos(PI * t));
+}
+double fus_zc(const a3d_shape& a, double x) { // src/aircraft.js:73
+  return x <= a.fus_xt0 ? 0 : a.fus_tailUp * a.fus_R0 * std::pow((x - a.fus_xt0) / a.fus_Lt, 2);
+}
+bool inLift(const a3d_surface& S, double x, double ay, double z) {  // src/air_field.js:115-123
+  const double* bx = S.bb;
+  if (x < bx[0] || x > bx[1] || z < bx[2] || z > bx[3] || ay > S.semi) return false;
+  double c = surf_chord(S, ay), xl = surf_xLE(S, ay), xc = (x - xl) / c;
+  if (xc < 0 || xc > 1) return false;
+  double th = nacaT(surf_tc(S, ay), xc) * c * (ay >= S.semi - 1e-6 ? 0 : 1);
+  double cam = nacaC(S.camber, xc) * c, shear = -(xc - 0.25) * c * S.tanI_deg;
+  double zm = S.z0 + (ay - S.sA) * S.tanD_deg + cam + shear;
+  return z >= zm - th && z <= zm + th;
+}
+bool inVt(const a3d_surface& V, double x, double ay, double z) {    // src/air_field.js:124-130
+  double s = z - V.z0;
+  if (s < -0.5 || s > V.semi) return false;
+  double ss = std::max(0.0, s), c = surf_chord(V, ss), xl = surf_xLE(V, ss), xc = (x - xl) / c;
+  if (xc < 0 || xc > 1) return false;
+  return ay <= nacaT(surf_tc(V, ss), xc) * c;
+}
+bool inFus(const a3d_shape& a, double x, double ay, double z) {    // src/air_field.js:131-134
+  if (x < 0 || x > a.fus_L) return false;
+  double R = fus_R(a, x), dz = z - fus_zc(a, x);
+  return ay * ay + dz * dz <= R * R;
+}
+
+struct GeomCtx {
+  const a3d_shape* a;
+  bool volW, volH, volV;
+  double hp0, hp1, cR, sR, dR;
+};
+
+bool solidAt(const GeomCtx& g, double x, double y, double z) {     // src/air_cfd.js:60-67
+  const a3d_shape& a = *g.a;
+  double ay = std::fabs(y);
+  for (int e = 0; e < a.n_engines; e++) {
+    const a3d_engine& v = a.engines[e];
+    if (v.internal || v.env_n == 0) continue;
+    double xe = x - v.x0;
+    if (xe < 0 || xe > v.env_xmax) continue;
+    double f = xe / v.env_xmax * v.env_n;
+    int k = std::min(v.env_n - 1, (int)std::floor(f));
+    double r = (double)v.env_R[k] + ((double)v.env_R[k + 1] - (double)v.env_R[k]) * (f - k);
+    if (std::hypot(ay - v.y, z - v.z) < r) return true;
+  }
+  if (inFus(a, x, ay, z)) return true;
+  if (g.volW && ay >= a.wing.sA * 0.9 && inLift(a.wing, x, ay, z)) return true;
+  if (g.volH && ay >= a.htail.sA * 0.9) {
+    double dx = x - g.hp0, dz = z - g.hp1;
+    if (inLift(a.htail, g.hp0 + dx * g.cR - dz * g.sR, ay, g.hp1 + dx * g.sR + dz * g.cR)) return true;
+  }
+  return g.volV && inVt(a.vtail, x, ay, z);
+}
+
+/* ---------------- grid ---------------- */
+std::vector<double> cfdAxis(double c0, double c1, double h, double lo, double hi, double r) {  // src/air_cfd.js:14-20
+  int n = (int)std::max(1.0, js_round((c1 - c0) / h));
+  double hh = (c1 - c0) / n;
+  std::vector<double> f;
+  for (int i = 0; i <= n; i++) f.push_back(c0 + i * hh);
+  if (lo < c0 - 1e-9) {
+    double d = hh, x = c0;
+    std::vector<double> L;
+    while (x > lo + 1e-9) { d *= r; x -= d; L.push_back(x); }
+    L.back() = lo;
+    size_t m = L.size();
+    if (m > 1 && (L[m - 2] - lo) < 0.5 * (m > 2 ? L[m - 3] - L[m - 2] : hh)) L.erase(L.begin() + (m - 2));
+    std::reverse(L.begin(), L.end());
+    f.insert(f.begin(), L.begin(), L.end());
+  }
+  if (hi > c1 + 1e-9) {
+    double d = hh, x = c1;
+    std::vector<double> R;
+    while (x < hi - 1e-9) { d *= r; x += d; R.push_back(x); }
+    R.back() = hi;
+    size_t m = R.size();
+    if (m > 1 && (hi - R[m - 2]) < 0.5 * (m > 2 ? R[m - 2] - R[m - 3] : hh)) R.erase(R.begin() + (m - 2));
+    f.insert(f.end(), R.begin(), R.end());
+  }
+  return f;
+}
+
+struct Grid {
+  int NX, NY, NZ;
+  long N;
+  std::vector<double> Xf, Yf, Zf;
+  std::vector<float> Xc, Yc, Zc, Xd, Yd, Zd;
+  double h;
+};
+
+void grid_from_faces(Grid& G, const int32_t dims[3], const double* xf, const double* yf, const double* zf) {
+  G.NX = dims[0]; G.NY = dims[1]; G.NZ = dims[2];
+  G.N = (long)G.NX * G.NY * G.NZ;
+  G.Xf.assign(xf, xf + G.NX + 1); G.Yf.assign(yf, yf + G.NY + 1); G.Zf.assign(zf, zf + G.NZ + 1);
+  auto mk = [](const std::vector<double>& f, std::vector<float>& c, std::vector<float>& d) {  // src/air_cfd.js:36
+    size_t n = f.size() - 1;
+    c.resize(n); d.resize(n);
+    for (size_t i = 0; i < n; i++) { c[i] = (float)(0.5 * (f[i] + f[i + 1])); d[i] = (float)(f[i + 1] - f[i]); }
+  };
+  mk(G.Xf, G.Xc, G.Xd); mk(G.Yf, G.Yc, G.Yd); mk(G.Zf, G.Zc, G.Zd);
+}
+
+}  // namespace
+
+extern "C" {
+
+int ref_grid_build(const a3d_shape* sh, double target, int32_t cap, double* xf, double* yf, double* zf,
+                   int32_t dims[3], double* h_out, double core_out[5]) {       // src/air_cfd.js:21-44
+  const a3d_shape& a = *sh;
+  const a3d_surface &w = a.wing, &ht = a.htail, &vt = a.vtail;
+  double L = a.fus_L, Lc = std::max(L, a.ref_b);
+  double x0 = -0.02 * L, x1 = std::max(std::max(L, surf_xLE(ht, ht.semi) + ht.ct), surf_xLE(vt, vt.semi) + vt.ct) + 0.03 * L;
+  double y1 = std::max(w.semi, ht.semi) + 0.03 * Lc, z0 = -a.fus_R0 - 0.03 * L, z1 = vt.z0 + vt.semi + 0.02 * L;
+  for (int e = 0; e < a.n_engines; e++) {
+    const a3d_engine& E = a.engines[e];
+    x0 = std::min(x0, E.x0 - 0.02 * L);
+    x1 = std::max(x1, E.x0 + a.exits[a.n_exits - 1].x + 0.05 * L);
+    if (!E.internal) { y1 = std::max(y1, E.y + a.view_Rmax + 0.03 * Lc); z0 = std::min(z0, E.z - a.view_Rmax - 0.03 * L); }
+  }
+  {  // w.pt(w.semi, 0.5, 0, 0)[2]  (src/aircraft.js:90-97)
+    double s = w.semi, c = surf_chord(w, s);
+    double th = nacaT(surf_tc(w, s), 0.5) * c, cam = nacaC(w.camber, 0.5) * c, shear = -(0.5 - 0.25) * c * w.tanI_pt;
+    double zt = w.z0 + (s - 0) * w.tanD_pt + cam + shear + 0 * th;
+    z0 = std::min(std::min(z0, zt - 0.05 * L), ht.z0 - 0.05 * L);
+  }
+  double lx0 = x0 - 0.55 * Lc, lx1 = x1 + 0.9 * Lc, ly1 = y1 + 0.6 * Lc, lz0 = z0 - 0.6 * Lc, lz1 = z1 + 0.6 * Lc;
+  const double r = 1.14;
+  double h = std::cbrt((x1 - x0) * y1 * (z1 - z0) / (target * 0.6));
+  std::vector<double> ax[3];
+  for (int it = 0; it < 6; it++) {
+    ax[0] = cfdAxis(x0, x1, h, lx0, lx1, r); ax[1] = cfdAxis(0, y1, h, 0, ly1, r); ax[2] = cfdAxis(z0, z1, h, lz0, lz1, r);
+    double n = (double)(ax[0].size() - 1) * (double)(ax[1].size() - 1) * (double)(ax[2].size() - 1);
+    h *= std::cbrt(n / target);
+    if (std::fabs(n / target - 1) < 0.04) break;
+  }
+  ax[0] = cfdAxis(x0, x1, h, lx0, lx1, r); ax[1] = cfdAxis(0, y1, h, 0, ly1, r); ax[2] = cfdAxis(z0, z1, h, lz0, lz1, r);
+  for (int d = 0; d < 3; d++) if ((int32_t)ax[d].size() > cap) return A3D_ERR_ARG;
+  std::copy(ax[0].begin(), ax[0].end(), xf); std::copy(ax[1].begin(), ax[1].end(), yf); std::copy(ax[2].begin(), ax[2].end(), zf);
+  dims[0] = (int32_t)ax[0].size() - 1; dims[1] = (int32_t)ax[1].size() - 1; dims[2] = (int32_t)ax[2].size() - 1;
+  *h_out = h;
+  core_out[0] = x0; core_out[1] = x1; core_out[2] = y1; core_out[3] = z0; core_out[4] = z1;
+  return 0;
+}
+
+int ref_geom_build(const a3d_shape* sh, const int32_t dims[3], const double* xf, const double* yf, const double* zf,
+                   double h, double delta_deg, uint8_t* t, float* phi, float* ap0, float* ap1, float* ap2, float* ap3,
+                   int64_t counts[2], int32_t vol[3]) {                           // src/air_cfd.js:50-141
+  Grid G; grid_from_faces(G, dims, xf, yf, zf);
+  const a3d_shape& a = *sh;
+  const int NX = G.NX, NY = G.NY, NZ = G.NZ; const long N = G.N;
+  GeomCtx c; c.a = sh;
+  const a3d_surface& ht = a.htail;
+  c.dR = (delta_deg) * DEG;
+  c.hp0 = surf_xLE(ht, 0) + 0.25 * ht.cr; c.hp1 = ht.z0; c.cR = std::cos(c.dR); c.sR = std::sin(c.dR);
+  auto thick = [&](const a3d_surface& S) { return 0.5 * (S.tcR * S.cr + S.tcT * S.ct) >= 1.5 * h; };
+  c.volW = thick(a.wing); c.volH = thick(ht); c.volV = thick(a.vtail);
+  const long NX1 = NX + 1, NXY1 = NX1 * (NY + 1);
+  std::vector<uint8_t> cin(NXY1 * (NZ + 1));
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int k = 0; k <= NZ; k++) for (int j = 0; j <= NY; j++) for (int i = 0; i <= NX; i++)
+    cin[k * NXY1 + j * NX1 + i] = solidAt(c, G.Xf[i], G.Yf[j], G.Zf[k]) ? 1 : 0;
+  auto cn = [&](int i, int j, int k) { return (int)cin[k * NXY1 + j * NX1 + i]; };
+  float* ap[4] = {ap0, ap1, ap2, ap3};
+  for (long q = 0; q < N; q++) { ap0[q] = 1; ap1[q] = 1; ap2[q] = 1; ap3[q] = 0; t[q] = 0; }
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int k = 0; k < NZ; k++) for (int j = 0; j < NY; j++) for (int i = 0; i < NX; i++) {
+    long q = ((long)k * NY + j) * NX + i;
+    int s = 0;
+    for (int cc = 0; cc < 8; cc++) s += cn(i + (cc & 1), j + ((cc >> 1) & 1), k + (cc >> 2));
+    if (s == 0) phi[q] = 1;
+    else if (s == 8) phi[q] = 0;
+    else {
+      int n = 0;
+      for (double aa : SUB) for (double bb : SUB) for (double c3 : SUB)
+        if (!solidAt(c, G.Xf[i] + aa * G.Xd[i], G.Yf[j] + bb * G.Yd[j], G.Zf[k] + c3 * G.Zd[k])) n++;
+      phi[q] = (float)(n / 27.0);
+    }
+    for (int d = 0; d < 3; d++) {
+      int fc[4][3];
+      if (d == 0) { int v[4][3] = {{i + 1, j, k}, {i + 1, j + 1, k}, {i + 1, j, k + 1}, {i + 1, j + 1, k + 1}}; std::memcpy(fc, v, sizeof v); }
+      else if (d == 1) { int v[4][3] = {{i, j + 1, k}, {i + 1, j + 1, k}, {i, j + 1, k + 1}, {i + 1, j + 1, k + 1}}; std::memcpy(fc, v, sizeof v); }
+      else { int v[4][3] = {{i, j, k + 1}, {i + 1, j, k + 1}, {i, j + 1, k + 1}, {i + 1, j + 1, k + 1}}; std::memcpy(fc, v, sizeof v); }
+      int m = 0;
+      for (auto& f : fc) m += cn(f[0], f[1], f[2]);
+      if (m == 0) continue;
+      if (m == 4) { ap[d][q] = 0; continue; }
+      int n = 0;
+      for (double aa : SUB) for (double bb : SUB) {
+        double x = d == 0 ? G.Xf[i + 1] : G.Xf[i] + aa * G.Xd[i];
+        double y = d == 1 ? G.Yf[j + 1] : G.Yf[j] + (d == 0 ? aa : bb) * G.Yd[j];
+        double z = d == 2 ? G.Zf[k + 1] : G.Zf[k] + bb * G.Zd[k];
+        if (!solidAt(c, x, y, z)) n++;
+      }
+      ap[d][q] = (float)(n / 9.0);
+    }
+  }
+  // thin-wing baffles (src/air_cfd.js:92-112)
+  auto zMean = [&](const a3d_surface& S, double sA, double x, double ay, bool& ok) -> double {
+    ok = false;
+    if (ay > S.semi || ay < sA) return 0;
+    double cc = surf_chord(S, ay), xc = (x - surf_xLE(S, ay)) / cc;
+    if (xc < 0 || xc > 1) return 0;
+    ok = true;
+    return S.z0 + (ay - sA) * S.tanD_deg + nacaC(S.camber, xc) * cc - (xc - 0.25) * cc * S.tanI_deg;
+  };
+  auto baffle = [&](const a3d_surface& S, double sA, bool rot) {
+    for (int j = 0; j < NY; j++) {
+      if (G.Yf[j] > S.semi || G.Yf[j + 1] < sA) continue;
+      for (int i = 0; i < NX; i++) {
+        int cov = 0; double zs = 0, ss = 0;
+        for (double aa : SUB) for (double bb : SUB) {
+          double x = G.Xf[i] + aa * G.Xd[i], y = G.Yf[j] + bb * G.Yd[j];
+          bool okm, ok1, ok0;
+          double zm = zMean(S, sA, x, y, okm);
+          if (!okm) continue;
+          double e = 0.02 * surf_chord(S, std::min(y, S.semi));
+          double z1 = zMean(S, sA, x + e, y, ok1), z0 = zMean(S, sA, x - e, y, ok0);
+          double sl = (ok1 && ok0) ? (z1 - z0) / (2 * e) : ok1 ? (z1 - zm) / e : ok0 ? (zm - z0) / e : 0;
+          if (rot) { zm -= (x - c.hp0) * std::tan(c.dR); sl -= std::tan(c.dR); }
+          cov++; zs += zm; ss += sl;
+        }
+        if (!cov) continue;
+        double zm = zs / cov;
+        int k = 0;
+        while (k < NZ - 2 && (double)G.Zc[k + 1] <= zm) k++;
+        long q = ((long)k * NY + j) * NX + i;
+        ap2[q] = (float)std::min((double)ap2[q], 1 - cov / 9.0);
+        ap3[q] = (float)(ss / cov);
+      }
+    }
+  };
+  baffle(a.wing, a.wing.sA, false);
+  baffle(ht, ht.sA, true);
+  for (long q = 0; q < N; q++) t[q] = phi[q] < 0.2 ? 1 : 0;                      // src/air_cfd.js:114
+  // fixed-state cells (src/air_cfd.js:118-131)
+  struct Fx { long q; int s; };
+  std::vector<Fx> fixed;
+  auto layerAt = [&](double xv) { int i = 0; while (i < NX - 1 && G.Xf[i + 1] <= xv) i++; return i; };
+  for (int e = 0; e < a.n_engines; e++) {
+    const a3d_engine& E = a.engines[e];
+    for (int x = 0; x < a.n_exits; x++) {
+      const a3d_exit& ex = a.exits[x];
+      int ty = ex.type, i = layerAt(E.x0 + ex.x - 1e-3);
+      auto mark = [&](double pad) {
+        int n = 0;
+        for (int k = 0; k < NZ; k++) for (int j = 0; j < NY; j++) {
+          double r = std::hypot((double)G.Yc[j] - E.y, (double)G.Zc[k] - E.z);
+          if (r <= ex.R + pad && r >= ex.Rin - pad) {
+            long q = ((long)k * NY + j) * NX + i; t[q] = (uint8_t)ty; phi[q] = 1; fixed.push_back({q, 1}); n++;
+          }
+        }
+        return n;
+      };
+      if (!mark(0)) mark(0.55 * std::max(std::max((double)G.Yd[0], (double)G.Zd[0]), h));
+    }
+    if (!E.internal) {
+      int i = layerAt(E.x0 + a.lip_x + 1e-3);
+      auto mark = [&](double pad) {
+        int n = 0;
+        for (int k = 0; k < NZ; k++) for (int j = 0; j < NY; j++) {
+          double r = std::hypot((double)G.Yc[j] - E.y, (double)G.Zc[k] - E.z);
+          if (r <= 0.9 * a.lip_r + pad) { long q = ((long)k * NY + j) * NX + i; t[q] = 3; phi[q] = 1; fixed.push_back({q, -1}); n++; }
+        }
+        return n;
+      };
+      if (!mark(0)) mark(0.55 * h);
+    }
+  }
+  // face clean-up next to solids (src/air_cfd.js:132-136)
+  const long NXY = (long)NX * NY;
+#pragma omp parallel for schedule(static)
+  for (int k = 0; k < NZ; k++) for (int j = 0; j < NY; j++) for (int i = 0; i < NX; i++) {
+    long q = ((long)k * NY + j) * NX + i;
+    for (int d = 0; d < 3; d++) {
+      bool inDom = d == 0 ? i + 1 < NX : d == 1 ? j + 1 < NY : k + 1 < NZ;
+      if (!inDom) { if (d == 2) ap3[q] = 0; continue; }
+      long q2 = d == 0 ? q + 1 : d == 1 ? q + NX : q + NXY;
+      if (t[q] == 1 || t[q2] == 1) { ap[d][q] = 0; if (d == 2) ap3[q] = 0; }
+    }
+    if (t[q] >= 3 || (k + 1 < NZ && t[q + NXY] >= 3)) ap3[q] = 0;
+  }
+  // outflow / inflow faces of fixed cells forced open (src/air_cfd.js:138)
+  for (const Fx& f : fixed) {
+    if (f.s > 0) { long q2 = f.q + 1; if (q2 < N && t[q2] == 0) ap0[f.q] = 1; }
+    else { long q0 = f.q - 1; if (q0 >= 0 && t[q0] == 0) ap0[q0] = 1; }
+  }
+  int64_t nS = 0, nC = 0;
+  for (long q = 0; q < N; q++) {
+    if (t[q] == 1) nS++;
+    else if (t[q] == 0 && (phi[q] < 1 || ap0[q] < 1 || ap1[q] < 1 || ap2[q] < 1)) nC++;
+  }
+  if (counts) { counts[0] = nS; counts[1] = nC; }
+  if (vol) { vol[0] = c.volW; vol[1] = c.volH; vol[2] = c.volV; }
+  return 0;
+}
+
+int64_t ref_force_list(const int32_t dims[3], const double* xf, const double* yf, const double* zf,
+                       const uint8_t* t, const float* ap0, const float* ap2, int64_t cap,
+                       int64_t* qo, double* cxo, double* czo, double* xo, double* zo) {  // src/air_cfd.js:143-152
+  Grid G; grid_from_faces(G, dims, xf, yf, zf);
+  const long NX = G.NX, NXY = NX * G.NY;
+  int64_t n = 0;
+  for (int k = 0; k < G.NZ; k++) for (int j = 0; j < G.NY; j++) for (int i = 0; i < G.NX; i++) {
+    long q = ((long)k * G.NY + j) * NX + i;
+    if (t[q] != 0) continue;
+    double axm = i > 0 ? (double)ap0[q - 1] : 1, azm = k > 0 ? (double)ap2[q - NXY] : 1;
+    double cx = ((double)ap0[q] - axm) * (double)G.Yd[j] * (double)G.Zd[k];
+    double cz = ((double)ap2[q] - azm) * (double)G.Xd[i] * (double)G.Yd[j];
+    if (cx != 0 || cz != 0) {
+      if (n < cap) { qo[n] = q; cxo[n] = cx; czo[n] = cz; xo[n] = G.Xc[i]; zo[n] = G.Zc[k]; }
+      n++;
+    }
+  }
+  return n;
+}
+
+}  // extern "C"
+
+/* ===================================================================================
+ * CfdCPU (src/air_cfd.js:157-259), templated on the state storage type.
+ * =================================================================================== */
+namespace {
+
+void cfdPrim5(double a0, double a1, double a2, double a3, double a4, double* o) {  // src/air_cfd.js:169
+  double r = std::max(a0, 1e-6), u = a1 / r, v = a2 / r, w = a3 / r;
+  o[0] = r; o[1] = u; o[2] = v; o[3] = w;
+  o[4] = std::max((CG - 1) * (a4 - 0.5 * r * (u * u + v * v + w * w)), 1e-7);
+}
+
+void cfdHLLC(const double* L, const double* R, int d, double* out) {  // src/air_cfd.js:179-195
+  const double gm = CG - 1, rL = L[0], rR = R[0], pL = L[4], pR = R[4], uL = L[1 + d], uR = R[1 + d];
+  const double aL = std::sqrt(CG * pL / rL), aR = std::sqrt(CG * pR / rR);
+  const double EL = pL / gm + 0.5 * rL * (L[1] * L[1] + L[2] * L[2] + L[3] * L[3]);
+  const double ER = pR / gm + 0.5 * rR * (R[1] * R[1] + R[2] * R[2] + R[3] * R[3]);
+  const double SL = std::min(uL - aL, uR - aR), SR = std::max(uL + aL, uR + aR);
+  if (SL >= 0 || SR <= 0) {
+    const double* K = SL >= 0 ? L : R;
+    double uK = K[1 + d], E = SL >= 0 ? EL : ER;
+    out[0] = K[0] * uK; out[1] = K[0] * K[1] * uK; out[2] = K[0] * K[2] * uK; out[3] = K[0] * K[3] * uK;
+    out[1 + d] += K[4];
+    out[4] = uK * (E + K[4]);
+    return;
+  }
+  const double SM = (pR - pL + rL * uL * (SL - uL) - rR * uR * (SR - uR)) / (rL * (SL - uL) - rR * (SR - uR));
+  const double *K; double S, uK, rK, pK, EK;
+  if (SM >= 0) { K = L; S = SL; uK = uL; rK = rL; pK = pL; EK = EL; } else { K = R; S = SR; uK = uR; rK = rR; pK = pR; EK = ER; }
+  const double f = rK * (S - uK) / (S - SM);
+  double Fm[4] = {rK * uK, rK * K[1] * uK, rK * K[2] * uK, rK * K[3] * uK};
+  Fm[1 + d] += pK;
+  double Um[4] = {rK, rK * K[1], rK * K[2], rK * K[3]}, Us[4] = {f, f * K[1], f * K[2], f * K[3]};
+  Us[1 + d] = f * SM;
+  const double Es = f * (EK / rK + (SM - uK) * (SM + pK / (rK * (S - uK))));
+  for (int c = 0; c < 4; c++) out[c] = Fm[c] + S * (Us[c] - Um[c]);
+  out[4] = uK * (EK + pK) + S * (Es - EK);
+}
+
+inline double mmod(double a, double b) { return a * b <= 0 ? 0 : std::fabs(a) < std::fabs(b) ? a : b; }  // src/air_cfd.js:196
+
+template <typename ST>
+struct RefSolver {
+  Grid G;
+  std::vector<uint8_t> t;
+  std::vector<float> phi, ap[4];
+  std::vector<ST> buf[3][5];
+  std::vector<ST>* Q; std::vector<ST>* B; std::vector<ST>* S1;
+  std::vector<double> W[5], dts;
+  double F[5], fix[3][5], cfl = 0.7;
+  int order = 2;
+  long it = 0;
+  int nthreads = 1;
+  std::vector<float> prevR; long prevIt = 0; bool havePrev = false;
+
+  RefSolver() {
+    Q = buf[0]; B = buf[1]; S1 = buf[2];
+    const double F0[5] = {1, 0, 0, 0, 1 / (CG * (CG - 1))};
+    for (int c = 0; c < 5; c++) { F[c] = F0[c]; fix[0][c] = fix[1][c] = fix[2][c] = F0[c]; }
+  }
+  void init() {
+    for (int b = 0; b < 3; b++) for (int c = 0; c < 5; c++) buf[b][c].assign(G.N, 0);
+    for (int c = 0; c < 5; c++) W[c].assign(G.N, 0);
+    dts.assign(G.N, 0);
+  }
+  void reset() { for (long q = 0; q < G.N; q++) for (int c = 0; c < 5; c++) Q[c][q] = (ST)F[c]; it = 0; }  // src/air_cfd.js:168
+
+  void prims(std::vector<ST>* Qs) {                                         // src/air_cfd.js:170-177
+    const long N = G.N;
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+    for (long q = 0; q < N; q++) {
+      double tmp[5];
+      if (t[q] >= 3) { const double* f = fix[t[q] - 3]; cfdPrim5(f[0], f[1], f[2], f[3], f[4], tmp); }
+      else cfdPrim5((double)Qs[0][q], (double)Qs[1][q], (double)Qs[2][q], (double)Qs[3][q], (double)Qs[4][q], tmp);
+      for (int c = 0; c < 5; c++) W[c][q] = tmp[c];
+    }
+  }
+
+  void cellResidual(int i, int j, int k, double* R) const {                // src/air_cfd.js:198-236
+    const int NX = G.NX, NY = G.NY, NZ = G.NZ;
+    const bool o2 = order == 2;
+    const long q0 = ((long)k * NY + j) * NX + i;
+    double P[25], A[4], s[15], L[5], Rr[5], fl[5];
+    int T[5];
+    for (int c = 0; c < 5; c++) R[c] = 0;
+    const double pC = W[4][q0];
+    for (int d = 0; d < 3; d++) {
+      const long st = d == 0 ? 1 : d == 1 ? NX : (long)NX * NY;
+      const int ic = d == 0 ? i : d == 1 ? j : k, nd = d == 0 ? NX : d == 1 ? NY : NZ;
+      const double h = d == 0 ? (double)G.Xd[i] : d == 1 ? (double)G.Yd[j] : (double)G.Zd[k];
+      const float* apd = ap[d].data();
+      for (int m = -2; m <= 2; m++) {
+        const int c = ic + m, o = 5 * (m + 2);
+        if (c >= nd || (c < 0 && d != 1)) { T[m + 2] = -1; cfdPrim5(F[0], F[1], F[2], F[3], F[4], P + o); continue; }
+        if (c < 0) { const long qm = q0 + (long)(-1 - c - ic) * st; T[m + 2] = -2; for (int v = 0; v < 5; v++) P[o + v] = W[v][qm]; P[o + 2] = -P[o + 2]; continue; }
+        const long q = q0 + m * st; T[m + 2] = t[q]; for (int v = 0; v < 5; v++) P[o + v] = W[v][q];
+      }
+      for (int m = -2; m <= 1; m++) { const int c = ic + m; A[m + 2] = (c < 0 || c >= nd) ? 1 : (double)apd[q0 + m * st]; }
+      for (int x = -1; x <= 1; x++) {
+        const bool ok = o2 && T[x + 1] == 0 && T[x + 2] == 0 && T[x + 3] == 0 && A[x + 1] == 1 && A[x + 2] == 1;
+        for (int v = 0; v < 5; v++) s[5 * (x + 1) + v] = ok ? mmod(P[5 * (x + 2) + v] - P[5 * (x + 1) + v], P[5 * (x + 3) + v] - P[5 * (x + 2) + v]) : 0;
+      }
+      for (int sg = 1; sg >= -1; sg -= 2) {
+        const double a = sg > 0 ? A[2] : A[1];
+        if (a <= 0) continue;
+        const int lo = sg > 0 ? 0 : -1;
+        for (int v = 0; v < 5; v++) { L[v] = P[5 * (lo + 2) + v] + 0.5 * s[5 * (lo + 1) + v]; Rr[v] = P[5 * (lo + 3) + v] - 0.5 * s[5 * (lo + 2) + v]; }
+        if (L[0] <= 0 || L[4] <= 0 || Rr[0] <= 0 || Rr[4] <= 0)
+          for (int v = 0; v < 5; v++) { L[v] = P[5 * (lo + 2) + v]; Rr[v] = P[5 * (lo + 3) + v]; }
+        cfdHLLC(L, Rr, d, fl);
+        for (int c = 0; c < 5; c++) R[c] -= sg * a * fl[c] / h;
+      }
+      R[1 + d] += pC * (A[2] - A[1]) / h;
+      if (d == 2) {
+        const double sUp = ap[3][q0], sDn = k > 0 ? (double)ap[3][q0 - (long)NX * NY] : 0;
+        if (sUp != 0 || sDn != 0) {
+          const double r = W[0][q0], u = W[1][q0], v = W[2][q0], w = W[3][q0];
+          const double Hh = (pC / (CG - 1) + 0.5 * r * (u * u + v * v + w * w) + pC) / r;
+          const double m = (sDn != 0 ? (1 - A[1]) * r * u * sDn : 0) - (sUp != 0 ? (1 - A[2]) * r * u * sUp : 0);
+          R[0] += m / h; R[1] += m * u / h; R[2] += m * v / h; R[3] += m * w / h; R[4] += m * Hh / h;
+        }
+      }
+    }
+    const double ph = phi[q0];
+    for (int c = 0; c < 5; c++) R[c] /= ph;
+  }
+
+  void stage(std::vector<ST>* Qin, std::vector<ST>* Bse, std::vector<ST>* Out, double wa, double wb, bool first) {  // src/air_cfd.js:237-251
+    prims(Qin);
+    const int NX = G.NX, NY = G.NY, NZ = G.NZ;
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+    for (int k = 0; k < NZ; k++) {
+      double R[5];
+      for (int j = 0; j < NY; j++) for (int i = 0; i < NX; i++) {
+        const long q = ((long)k * NY + j) * NX + i;
+        if (t[q] != 0) {
+          if (t[q] >= 3) { const double* f = fix[t[q] - 3]; for (int c = 0; c < 5; c++) Out[c][q] = (ST)f[c]; }
+          else for (int c = 0; c < 5; c++) Out[c][q] = Bse[c][q];
+          continue;
+        }
+        if (first) {
+          const double a = std::sqrt(CG * W[4][q] / W[0][q]);
+          dts[q] = cfl * std::max((double)phi[q], 0.25) / ((std::fabs(W[1][q]) + a) / (double)G.Xd[i] + (std::fabs(W[2][q]) + a) / (double)G.Yd[j] + (std::fabs(W[3][q]) + a) / (double)G.Zd[k]);
+        }
+        cellResidual(i, j, k, R);
+        const double dt = dts[q];
+        for (int c = 0; c < 5; c++) Out[c][q] = (ST)(wa * (double)Bse[c][q] + wb * ((double)Qin[c][q] + dt * R[c]));
+        const double r = std::max((double)Out[0][q], 1e-4);
+        Out[0][q] = (ST)r;
+        const double o1 = Out[1][q], o2 = Out[2][q], o3 = Out[3][q];
+        const double ke = 0.5 * (o1 * o1 + o2 * o2 + o3 * o3) / r;
+        if ((CG - 1) * ((double)Out[4][q] - ke) < 1e-5) Out[4][q] = (ST)(1e-5 / (CG - 1) + ke);
+      }
+    }
+  }
+  void step(int n) {                                                        // src/air_cfd.js:252-258
+    for (int s = 0; s < n; s++) {
+      stage(Q, Q, S1, 0, 1, true);
+      stage(S1, Q, B, 0.5, 0.5, false);
+      std::swap(Q, B);
+      it++;
+    }
+  }
+};
+
+template <typename ST>
+void forces_of(const RefSolver<ST>& s, double alpha, double M, double S, double xcg, double zcg, double cref, double* out) {
+  // cfdForceList + cfdForces (src/air_cfd.js:143-152, 443-452)
+  const Grid& G = s.G;
+  const long NX = G.NX, NXY = NX * G.NY;
+  double Fx = 0, Fz = 0, My = 0;
+  const double pinf = 1 / CG;
+  for (int k = 0; k < G.NZ; k++) for (int j = 0; j < G.NY; j++) for (int i = 0; i < G.NX; i++) {
+    long q = ((long)k * G.NY + j) * NX + i;
+    if (s.t[q] != 0) continue;
+    double axm = i > 0 ? (double)s.ap[0][q - 1] : 1, azm = k > 0 ? (double)s.ap[2][q - NXY] : 1;
+    double cx = ((double)s.ap[0][q] - axm) * (double)G.Yd[j] * (double)G.Zd[k];
+    double cz = ((double)s.ap[2][q] - azm) * (double)G.Xd[i] * (double)G.Yd[j];
+    if (!(cx != 0 || cz != 0)) continue;
+    double r = s.Q[0][q], u = (double)s.Q[1][q] / r, v = (double)s.Q[2][q] / r, w = (double)s.Q[3][q] / r;
+    double dp = (CG - 1) * ((double)s.Q[4][q] - 0.5 * r * (u * u + v * v + w * w)) - pinf;
+    double fx = -dp * cx, fz = -dp * cz;
+    Fx += fx; Fz += fz; My += ((double)G.Zc[k] - zcg) * fx - ((double)G.Xc[i] - xcg) * fz;
+  }
+  double a = alpha * DEG, qd = 0.5 * M * M, kk = 2 / (qd * S);
+  out[0] = kk * (Fz * std::cos(a) - Fx * std::sin(a));
+  out[1] = kk * (Fx * std::cos(a) + Fz * std::sin(a));
+  out[2] = kk * My / cref;
+}
+
+void cfdLocate(const std::vector<float>& c, double v, int& i, double& tx) {  // src/air_cfd.js:453
+  int n = (int)c.size();
+  if (v <= c[0]) { i = 0; tx = 0; return; }
+  if (v >= c[n - 1]) { i = n - 2; tx = 1; return; }
+  int lo = 0, hi = n - 1;
+  while (hi - lo > 1) { int m = (lo + hi) >> 1; if (c[m] <= v) lo = m; else hi = m; }
+  i = lo; tx = (v - (double)c[lo]) / ((double)c[hi] - (double)c[lo]);
+}
+
+template <typename ST>
+double trefftz_of(const RefSolver<ST>& s, double xT, double alpha, double M, double S) {  // src/air_cfd.js:560-570
+  const Grid& G = s.G;
+  int i0; double tx; cfdLocate(G.Xc, xT, i0, tx);
+  double a = alpha * DEG, ca = std::cos(a), sa = std::sin(a), Mn = std::max(M, 0.05), sum = 0;
+  for (int k = 0; k < G.NZ; k++) for (int j = 0; j < G.NY; j++) {
+    double u = 0, v = 0, w = 0, ws = 0;
+    for (int di = 0; di < 2; di++) {
+      long q = ((long)k * G.NY + j) * G.NX + i0 + di;
+      if (s.t[q] != 0) continue;
+      double ww = di ? tx : 1 - tx, r = s.Q[0][q];
+      u += ww * (double)s.Q[1][q] / r; v += ww * (double)s.Q[2][q] / r; w += ww * (double)s.Q[3][q] / r; ws += ww;
+    }
+    if (ws < 1e-6) continue;
+    u /= ws; v /= ws; w /= ws;
+    double vn = w * ca - u * sa;
+    sum += (v * v + vn * vn) * (double)G.Yd[j] * (double)G.Zd[k];
+  }
+  return 2 * sum / (Mn * Mn * S);
+}
+
+template <typename ST>
+double residual_of(RefSolver<ST>& s, int stride) {                          // src/air_cfd.js:552-555
+  const long N = s.G.N;
+  long nIt = s.it - s.prevIt;
+  double res = -1;
+  if (s.havePrev && nIt > 0) {
+    double sum = 0; long n = 0;
+    for (long q = 0; q < N; q += stride) {
+      if (s.t[q] != 0) continue;
+      double d = (double)s.Q[0][q] - (double)s.prevR[q];
+      sum += d * d; n++;
+    }
+    res = std::sqrt(sum / std::max(1L, n)) / nIt;
+  }
+  s.prevR.resize(N);
+  for (long q = 0; q < N; q++) s.prevR[q] = (float)s.Q[0][q];
+  s.prevIt = s.it; s.havePrev = true;
+  return res;
+}
+
+template <typename ST>
+double mmax_of(const RefSolver<ST>& s, int stride) {                          // src/air_cfd.js:571-572
+  double mMax = 0;
+  for (long q = 0; q < s.G.N; q += stride) {
+    if (s.t[q] != 0) continue;
+    double r = s.Q[0][q], u = (double)s.Q[1][q] / r, v = (double)s.Q[2][q] / r, w = (double)s.Q[3][q] / r;
+    double p = (CG - 1) * ((double)s.Q[4][q] - 0.5 * r * (u * u + v * v + w * w));
+    double m2 = (u * u + v * v + w * w) / (CG * p / r);
+    if (m2 > mMax) mMax = m2;
+  }
+  return std::sqrt(mMax);
+}
+
+template <typename ST>
+void write_state(RefSolver<ST>& s, const double* in) {
+  long N = s.G.N;
+  for (int c = 0; c < 5; c++) for (long q = 0; q < N; q++) s.Q[c][q] = (ST)in[c * N + q];
+}
+
+struct AnySolver {
+  int prec;  // 32 or 64
+  RefSolver<float>* s32 = nullptr;
+  RefSolver<double>* s64 = nullptr;
+};
+
+template <typename ST>
+void setup(RefSolver<ST>* s, const int32_t dims[3], const double* xf, const double* yf, const double* zf,
+           const uint8_t* t, const float* phi, const float* ap0, const float* ap1, const float* ap2, const float* ap3) {
+  grid_from_faces(s->G, dims, xf, yf, zf);
+  long N = s->G.N;
+  s->t.assign(t, t + N); s->phi.assign(phi, phi + N);
+  s->ap[0].assign(ap0, ap0 + N); s->ap[1].assign(ap1, ap1 + N); s->ap[2].assign(ap2, ap2 + N); s->ap[3].assign(ap3, ap3 + N);
+  s->init();
+}
+
+}  // namespace
+
+#define DISPATCH(h, expr) do { AnySolver* A_ = (AnySolver*)(h); if (A_->prec == 64) { auto* S_ = A_->s64; expr; } else { auto* S_ = A_->s32; expr; } } while (0)
+
+extern "C" {
+
+void* ref_solver_new(int prec, const int32_t dims[3], const double* xf, const double* yf, const double* zf,
+                     const uint8_t* t, const float* phi, const float* ap0, const float* ap1, const float* ap2, const float* ap3) {
+  AnySolver* A = new AnySolver();
+  A->prec = prec == 64 ? 64 : 32;
+  if (A->prec == 64) { A->s64 = new RefSolver<double>(); setup(A->s64, dims, xf, yf, zf, t, phi, ap0, ap1, ap2, ap3); }
+  else { A->s32 = new RefSolver<float>(); setup(A->s32, dims, xf, yf, zf, t, phi, ap0, ap1, ap2, ap3); }
+  return A;
+}
+void ref_solver_free(void* h) { AnySolver* A = (AnySolver*)h; delete A->s32; delete A->s64; delete A; }
+void ref_solver_threads(void* h, int n) { DISPATCH(h, S_->nthreads = std::max(1, n)); }
+void ref_solver_opt(void* h, double cfl, int order) { DISPATCH(h, (S_->cfl = cfl, S_->order = order)); }
+void ref_solver_set_free(void* h, const double* F) { DISPATCH(h, for (int c = 0; c < 5; c++) S_->F[c] = F[c]); }
+void ref_solver_set_fix(void* h, const double* fx) { DISPATCH(h, for (int c = 0; c < 15; c++) S_->fix[c / 5][c % 5] = fx[c]); }
+void ref_solver_reset(void* h) { DISPATCH(h, S_->reset()); }
+void ref_solver_step(void* h, int n) { DISPATCH(h, S_->step(n)); }
+long ref_solver_iterations(void* h) { long it = 0; DISPATCH(h, it = S_->it); return it; }
+void ref_solver_read(void* h, double* out) {  // 5*N doubles (exact copies of the stored values)
+  DISPATCH(h, { long N = S_->G.N; for (int c = 0; c < 5; c++) for (long q = 0; q < N; q++) out[c * N + q] = (double)S_->Q[c][q]; });
+}
+void ref_solver_write(void* h, const double* in) {  // 5*N doubles, rounded to the storage type
+  DISPATCH(h, write_state(*S_, in));
+}
+void ref_solver_forces(void* h, double alpha, double M, double S, double xcg, double zcg, double cref, double* out) {
+  DISPATCH(h, forces_of(*S_, alpha, M, S, xcg, zcg, cref, out));
+}
+double ref_solver_trefftz(void* h, double xT, double alpha, double M, double S) { double r = 0; DISPATCH(h, r = trefftz_of(*S_, xT, alpha, M, S)); return r; }
+double ref_solver_residual(void* h, int stride) { double r = 0; DISPATCH(h, r = residual_of(*S_, stride)); return r; }
+double ref_solver_mach_max(void* h, int stride) { double r = 0; DISPATCH(h, r = mmax_of(*S_, stride)); return r; }
+int ref_max_threads(void) {
+#ifdef _OPENMP
+  return omp_get_max_threads();
+#else
+  return 1;
+#endif
+}
+
+}  // extern "C"
