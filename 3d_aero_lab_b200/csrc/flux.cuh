@@ -1,0 +1,104 @@
+// flux.cuh - FP32 device arithmetic of the Euler step: primitives, minmod MUSCL
+// reconstruction and the HLLC flux (src/air_cfd.js:169-196, CFD3_FS 276-295).
+//
+// Faces are evaluated in a rotated frame: `un` is the velocity component normal to the
+// face, `u1`, `u2` the two tangential ones.  The HLLC formulas of the reference are
+// symmetric in the tangential components, so the rotation changes no arithmetic.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace a3d {
+
+constexpr float kG = 1.4f;
+constexpr float kGm = 1.4f - 1.0f;  // gamma - 1 as the float32 shader forms it
+
+struct Prim {
+  float r, un, u1, u2, p;
+};
+
+// Conservative -> primitive with the reference's floors rho >= 1e-6, p >= 1e-7
+// (cfdPrim5, src/air_cfd.js:169); output in the unrotated order (rho, u, v, w, p).
+__device__ __forceinline__ void cons_to_prim(float a0, float a1, float a2, float a3, float a4, float o[5]) {
+  const float r = fmaxf(a0, 1e-6f), ir = 1.0f / r;
+  const float u = a1 * ir, v = a2 * ir, w = a3 * ir;
+  o[0] = r; o[1] = u; o[2] = v; o[3] = w;
+  o[4] = fmaxf(kGm * (a4 - 0.5f * r * (u * u + v * v + w * w)), 1e-7f);
+}
+
+__device__ __forceinline__ float minmod(float a, float b) {  // mmod, src/air_cfd.js:196
+  return (a * b <= 0.f) ? 0.f : (fabsf(a) < fabsf(b) ? a : b);
+}
+
+// Rotate (rho, u, v, w, p) so that component d of the velocity becomes `un`.
+__device__ __forceinline__ Prim rot(const float P[5], int d) {
+  Prim o;
+  o.r = P[0]; o.p = P[4];
+  if (d == 0) { o.un = P[1]; o.u1 = P[2]; o.u2 = P[3]; }
+  else if (d == 1) { o.un = P[2]; o.u1 = P[1]; o.u2 = P[3]; }
+  else { o.un = P[3]; o.u1 = P[1]; o.u2 = P[2]; }
+  return o;
+}
+
+// HLLC flux with Davis wave-speed estimates (cfdHLLC, src/air_cfd.js:179-195).
+// Output: mass, normal momentum, tangential momenta, energy.
+__device__ __forceinline__ void hllc(const Prim& L, const Prim& R, float F[5]) {
+  const float aL = sqrtf(kG * L.p / L.r), aR = sqrtf(kG * R.p / R.r);
+  const float EL = L.p / kGm + 0.5f * L.r * (L.un * L.un + L.u1 * L.u1 + L.u2 * L.u2);
+  const float ER = R.p / kGm + 0.5f * R.r * (R.un * R.un + R.u1 * R.u1 + R.u2 * R.u2);
+  const float SL = fminf(L.un - aL, R.un - aR), SR = fmaxf(L.un + aL, R.un + aR);
+  if (SL >= 0.f || SR <= 0.f) {  // supersonic: upwind state flux
+    const bool left = SL >= 0.f;
+    const Prim& K = left ? L : R;
+    const float E = left ? EL : ER, m = K.r * K.un;
+    F[0] = m; F[1] = m * K.un + K.p; F[2] = m * K.u1; F[3] = m * K.u2; F[4] = K.un * (E + K.p);
+    return;
+  }
+  const float SM = (R.p - L.p + L.r * L.un * (SL - L.un) - R.r * R.un * (SR - R.un)) /
+                   (L.r * (SL - L.un) - R.r * (SR - R.un));
+  const bool left = SM >= 0.f;
+  const float rK = left ? L.r : R.r, uK = left ? L.un : R.un, v1 = left ? L.u1 : R.u1, v2 = left ? L.u2 : R.u2;
+  const float pK = left ? L.p : R.p, EK = left ? EL : ER, S = left ? SL : SR;
+  const float f = rK * (S - uK) / (S - SM);
+  const float m = rK * uK;
+  F[0] = m + S * (f - rK);
+  F[1] = m * uK + pK + S * (f * SM - m);
+  F[2] = m * v1 + S * (f * v1 - rK * v1);
+  F[3] = m * v2 + S * (f * v2 - rK * v2);
+  const float Es = f * (EK / rK + (SM - uK) * (SM + pK / (rK * (S - uK))));
+  F[4] = uK * (EK + pK) + S * (Es - EK);
+}
+
+// Flux through the face between cells b (left) and c (right) along one direction, with the
+// neighbours a (left of b) and e (right of c).  okL/okR: the slope test at b and c passed
+// (three fluid cells and both faces fully open, src/air_cfd.js:213-216).  Falls back to first
+// order when a reconstructed density or pressure is not positive (src/air_cfd.js:221).
+__device__ __forceinline__ void face_flux(const Prim& a, const Prim& b, const Prim& c, const Prim& e, bool okL,
+                                          bool okR, float F[5]) {
+  Prim L = b, R = c;
+  if (okL) {
+    L.r = b.r + 0.5f * minmod(b.r - a.r, c.r - b.r);
+    L.un = b.un + 0.5f * minmod(b.un - a.un, c.un - b.un);
+    L.u1 = b.u1 + 0.5f * minmod(b.u1 - a.u1, c.u1 - b.u1);
+    L.u2 = b.u2 + 0.5f * minmod(b.u2 - a.u2, c.u2 - b.u2);
+    L.p = b.p + 0.5f * minmod(b.p - a.p, c.p - b.p);
+  }
+  if (okR) {
+    R.r = c.r - 0.5f * minmod(c.r - b.r, e.r - c.r);
+    R.un = c.un - 0.5f * minmod(c.un - b.un, e.un - c.un);
+    R.u1 = c.u1 - 0.5f * minmod(c.u1 - b.u1, e.u1 - c.u1);
+    R.u2 = c.u2 - 0.5f * minmod(c.u2 - b.u2, e.u2 - c.u2);
+    R.p = c.p - 0.5f * minmod(c.p - b.p, e.p - c.p);
+  }
+  if (L.r <= 0.f || L.p <= 0.f || R.r <= 0.f || R.p <= 0.f) { L = b; R = c; }
+  hllc(L, R, F);
+}
+
+// Scatter a rotated-frame flux back to (mass, x-, y-, z-momentum, energy).
+__device__ __forceinline__ void unrot(const float F[5], int d, float o[5]) {
+  o[0] = F[0]; o[4] = F[4];
+  if (d == 0) { o[1] = F[1]; o[2] = F[2]; o[3] = F[3]; }
+  else if (d == 1) { o[1] = F[2]; o[2] = F[1]; o[3] = F[3]; }
+  else { o[1] = F[2]; o[2] = F[3]; o[3] = F[1]; }
+}
+
+}  // namespace a3d

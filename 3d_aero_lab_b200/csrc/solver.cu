@@ -1,0 +1,420 @@
+// solver.cu - the SSP-RK2 cut-cell Euler solver object (CfdCPU / CfdGPU, src/air_cfd.js:157-438).
+//
+// State: three structure-of-arrays float32 buffers Q, S1, B (rho, rho*u, rho*v, rho*w, E),
+// each component padded to a multiple of 64 cells.  One iteration is two stage launches:
+//   S1 = Q + dt R(Q)                         (stage 1, dt from Q)
+//   B  = 0.5 Q + 0.5 (S1 + dt R(S1))         (stage 2, dt again from Q)
+// followed by a buffer rotation Q <-> B (src/air_cfd.js:252-258).  dt is recomputed from
+// the base state Q in both stages, as the reference's shader does (CFD3_FS :357-359); it is
+// the value CfdCPU stores in stage 1 and reuses.
+//
+// Two stage kernels are built:
+//   KERNEL_CELL  - one thread per cell, six faces per cell, the reference's structure;
+//   KERNEL_MARCH - CTA tile of 32 x 8 columns marching in z, every face flux computed
+//                  once per tile and shared through shared memory (stage_march.cuh).
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+#include "flux.cuh"
+#include "solver.cuh"
+
+namespace a3d {
+
+namespace {
+
+// ----------------------------------------------------------------------------------------
+// per-cell codes: type, static slope-test bits, irregular and baffle flags
+// ----------------------------------------------------------------------------------------
+__global__ void k_codes(int NX, int NY, int NZ, const uint8_t* t, const float* phi, const float* ap0,
+                        const float* ap1, const float* ap2, const float* ap3, uint8_t* code) {
+  const long NXY = (long)NX * NY, N = NXY * NZ;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < N; q += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % NX), j = (int)((q / NX) % NY), k = (int)(q / NXY);
+    uint8_t c = t[q] & 7;
+    auto fluid = [&](long qq) { return t[qq] == T_FLUID; };
+    // slope allowed at this cell along d: both neighbours in the domain and fluid, this cell
+    // fluid, both faces fully open (src/air_cfd.js:214; out-of-domain ghosts are never fluid)
+    if (t[q] == T_FLUID) {
+      if (i > 0 && i + 1 < NX && fluid(q - 1) && fluid(q + 1) && ap0[q - 1] == 1.f && ap0[q] == 1.f) c |= C_OKX;
+      if (j > 0 && j + 1 < NY && fluid(q - NX) && fluid(q + NX) && ap1[q - NX] == 1.f && ap1[q] == 1.f) c |= C_OKY;
+      if (k > 0 && k + 1 < NZ && fluid(q - NXY) && fluid(q + NXY) && ap2[q - NXY] == 1.f && ap2[q] == 1.f) c |= C_OKZ;
+    }
+    if (phi[q] != 1.f || ap0[q] != 1.f || ap1[q] != 1.f || ap2[q] != 1.f) c |= C_IRR;
+    if (ap3[q] != 0.f || (k > 0 && ap3[q - NXY] != 0.f)) c |= C_BAF;
+    code[q] = c;
+  }
+}
+
+__global__ void k_fill(float* Q, long Np, long N, float f0, float f1, float f2, float f3, float f4) {
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < N; q += (long)gridDim.x * blockDim.x) {
+    Q[q] = f0; Q[Np + q] = f1; Q[2 * Np + q] = f2; Q[3 * Np + q] = f3; Q[4 * Np + q] = f4;
+  }
+}
+
+// ----------------------------------------------------------------------------------------
+// KERNEL_CELL: one thread per cell, the reference's per-cell structure.
+// ----------------------------------------------------------------------------------------
+
+// Primitive state of the stencil cell at (i, j, k) with the reference's ghost rules
+// (src/air_cfd.js:205-210): far field beyond the domain in x, z and +y, symmetry mirror
+// (v negated) below y = 0, fixed-state substitution for types 3-5.  Returns the type.
+__device__ __forceinline__ int stencil_prim(const StageArgs& a, int i, int j, int k, float P[5]) {
+  if (i < 0 || i >= a.NX || k < 0 || k >= a.NZ || j >= a.NY) {
+    for (int v = 0; v < 5; v++) P[v] = a.Pff[v];
+    return T_GHOST;
+  }
+  const bool mirror = j < 0;
+  const int jj = mirror ? -1 - j : j;
+  const long q = ((long)k * a.NY + jj) * a.NX + i;
+  const int t = a.code[q] & 7;
+  if (t >= T_SINK) { for (int v = 0; v < 5; v++) P[v] = a.Pfix[t - T_SINK][v]; }
+  else cons_to_prim(a.Qin[q], a.Qin[a.Np + q], a.Qin[2 * a.Np + q], a.Qin[3 * a.Np + q], a.Qin[4 * a.Np + q], P);
+  if (mirror) { P[2] = -P[2]; return T_MIRROR; }
+  return t;
+}
+
+__global__ void __launch_bounds__(256) k_stage_cell(StageArgs a) {
+  const long NXY = (long)a.NX * a.NY, N = NXY * a.NZ;
+  const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
+  if (q >= N) return;
+  const int i = (int)(q % a.NX), j = (int)((q / a.NX) % a.NY), k = (int)(q / NXY);
+  const uint8_t cq = a.code[q];
+  const int t = cq & 7;
+  const long Np = a.Np;
+  if (t != T_FLUID) {  // src/air_cfd.js:242
+    if (t >= T_SINK) for (int c = 0; c < 5; c++) a.Out[c * Np + q] = a.Ufix[t - T_SINK][c];
+    else for (int c = 0; c < 5; c++) a.Out[c * Np + q] = a.B[c * Np + q];
+    return;
+  }
+  float Pc[5];
+  cons_to_prim(a.Qin[q], a.Qin[Np + q], a.Qin[2 * Np + q], a.Qin[3 * Np + q], a.Qin[4 * Np + q], Pc);
+  const float pC = Pc[4];
+  float R[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+  const float* apd[3] = {a.ap0, a.ap1, a.ap2};
+  const long st[3] = {1, a.NX, NXY};
+  const int ic[3] = {i, j, k}, nd[3] = {a.NX, a.NY, a.NZ};
+  const float rh[3] = {a.rXd[i], a.rYd[j], a.rZd[k]};
+  float Aface[3][2];
+  for (int d = 0; d < 3; d++) {
+    Prim P[5];
+    bool fl[5];
+    for (int m = -2; m <= 2; m++) {
+      float W[5];
+      const int ii = i + (d == 0 ? m : 0), jj = j + (d == 1 ? m : 0), kk = k + (d == 2 ? m : 0);
+      const int tt = (m == 0) ? T_FLUID : stencil_prim(a, ii, jj, kk, W);
+      if (m == 0) for (int v = 0; v < 5; v++) W[v] = Pc[v];
+      P[m + 2] = rot(W, d);
+      fl[m + 2] = tt == T_FLUID;
+    }
+    float A[4];
+    for (int m = -2; m <= 1; m++) {
+      const int c = ic[d] + m;
+      A[m + 2] = (c < 0 || c >= nd[d]) ? 1.f : apd[d][q + m * st[d]];
+    }
+    bool ok[3];
+    for (int x = 0; x < 3; x++)
+      ok[x] = a.order2 && fl[x] && fl[x + 1] && fl[x + 2] && A[x] == 1.f && A[x + 1] == 1.f;
+    float F[5], G[5];
+    if (A[2] > 0.f) {  // + face
+      face_flux(P[1], P[2], P[3], P[4], ok[1], ok[2], F);
+      unrot(F, d, G);
+      for (int c = 0; c < 5; c++) R[c] -= A[2] * G[c] * rh[d];
+    }
+    if (A[1] > 0.f) {  // - face
+      face_flux(P[0], P[1], P[2], P[3], ok[0], ok[1], F);
+      unrot(F, d, G);
+      for (int c = 0; c < 5; c++) R[c] += A[1] * G[c] * rh[d];
+    }
+    R[1 + d] += pC * (A[2] - A[1]) * rh[d];  // wall-pressure source
+    Aface[d][0] = A[1];
+    Aface[d][1] = A[2];
+  }
+  if (cq & C_BAF) {  // baffle transpiration w = u dz/dx (src/air_cfd.js:226-233)
+    const float sUp = a.ap3[q], sDn = k > 0 ? a.ap3[q - NXY] : 0.f;
+    if (sUp != 0.f || sDn != 0.f) {
+      const float r = Pc[0], u = Pc[1], v = Pc[2], w = Pc[3];
+      const float Hh = (pC / kGm + 0.5f * r * (u * u + v * v + w * w) + pC) / r;
+      const float m = (sDn != 0.f ? (1.f - Aface[2][0]) * r * u * sDn : 0.f) - (sUp != 0.f ? (1.f - Aface[2][1]) * r * u * sUp : 0.f);
+      const float mh = m * rh[2];
+      R[0] += mh; R[1] += mh * u; R[2] += mh * v; R[3] += mh * w; R[4] += mh * Hh;
+    }
+  }
+  const float ph = (cq & C_IRR) ? a.phi[q] : 1.f;
+  if (ph != 1.f) { const float iph = 1.f / ph; for (int c = 0; c < 5; c++) R[c] *= iph; }
+  // local time step from the base state (src/air_cfd.js:243, CFD3_FS :357-359)
+  float Pb[5];
+  if (a.wa == 0.f) { for (int v = 0; v < 5; v++) Pb[v] = Pc[v]; }
+  else cons_to_prim(a.B[q], a.B[Np + q], a.B[2 * Np + q], a.B[3 * Np + q], a.B[4 * Np + q], Pb);
+  const float as = sqrtf(kG * Pb[4] / Pb[0]);
+  const float dt = a.cfl * fmaxf(ph, 0.25f) / ((fabsf(Pb[1]) + as) * rh[0] + (fabsf(Pb[2]) + as) * rh[1] + (fabsf(Pb[3]) + as) * rh[2]);
+  float o[5];
+  for (int c = 0; c < 5; c++) {
+    const float qin = a.Qin[c * Np + q];
+    o[c] = (a.wa == 0.f) ? (qin + dt * R[c]) : (a.wa * a.B[c * Np + q] + a.wb * (qin + dt * R[c]));
+  }
+  o[0] = fmaxf(o[0], 1e-4f);  // positivity clamps (src/air_cfd.js:247-249)
+  const float ke = 0.5f * (o[1] * o[1] + o[2] * o[2] + o[3] * o[3]) / o[0];
+  if (kGm * (o[4] - ke) < 1e-5f) o[4] = 1e-5f / kGm + ke;
+  for (int c = 0; c < 5; c++) a.Out[c * Np + q] = o[c];
+}
+
+int blocks_for(long work, int threads = 256) {
+  return (int)std::max(1L, std::min((work + threads - 1) / threads, 148L * 64));
+}
+
+void prim_of(const double U[5], float P[5]) {  // cfdPrim5 in float64, rounded to float32
+  const double r = std::max(U[0], 1e-6), u = U[1] / r, v = U[2] / r, w = U[3] / r;
+  P[0] = (float)r; P[1] = (float)u; P[2] = (float)v; P[3] = (float)w;
+  P[4] = (float)std::max((kGamma - 1) * (U[4] - 0.5 * r * (u * u + v * v + w * w)), 1e-7);
+}
+
+}  // namespace
+
+int launch_march(a3d_solver* s, const StageArgs& a);  // stage_march.cu
+
+void fill_stage_args(a3d_solver* s, StageArgs& a, const float* Qin, const float* B, float* Out, float wa, float wb) {
+  a.Qin = Qin; a.B = B; a.Out = Out; a.Np = s->Np;
+  a.code = s->code; a.phi = s->geo.phi; a.ap0 = s->geo.ap0; a.ap1 = s->geo.ap1; a.ap2 = s->geo.ap2; a.ap3 = s->geo.ap3;
+  a.rXd = s->grid.rXd; a.rYd = s->grid.rYd; a.rZd = s->grid.rZd;
+  a.NX = s->grid.NX; a.NY = s->grid.NY; a.NZ = s->grid.NZ;
+  a.wa = wa; a.wb = wb; a.cfl = (float)s->cfl; a.order2 = s->order == 2;
+  prim_of(s->F, a.Pff);
+  for (int f = 0; f < 3; f++) {
+    prim_of(s->fix[f], a.Pfix[f]);
+    for (int c = 0; c < 5; c++) a.Ufix[f][c] = (float)s->fix[f][c];
+  }
+}
+
+int launch_stage(a3d_solver* s, const StageArgs& a) {
+  if (s->kernel == KERNEL_MARCH) return launch_march(s, a);
+  k_stage_cell<<<(unsigned)((s->N + 255) / 256), 256, 0, s->st>>>(a);
+  A3D_CUDA(cudaGetLastError());
+  return A3D_OK;
+}
+
+int solver_finish_setup(a3d_solver* s) {
+  const long N = s->N;
+  s->Np = round_up(N, 64);
+  A3D_CUDA(cudaMalloc(&s->state, 3 * 5 * s->Np * sizeof(float)));
+  for (int b = 0; b < 3; b++) s->buf[b] = s->state + (long)b * 5 * s->Np;
+  A3D_CUDA(cudaMemsetAsync(s->state, 0, 3 * 5 * s->Np * sizeof(float), s->st));
+  A3D_CUDA(cudaMalloc(&s->code, round_up(N, 256)));
+  k_codes<<<blocks_for(N), 256, 0, s->st>>>(s->grid.NX, s->grid.NY, s->grid.NZ, s->geo.t, s->geo.phi, s->geo.ap0,
+                                            s->geo.ap1, s->geo.ap2, s->geo.ap3, s->code);
+  A3D_CUDA(cudaGetLastError());
+  A3D_CUDA(cudaMalloc(&s->d_red, 4096 * 8 * sizeof(double)));
+  A3D_CUDA(cudaMallocHost(&s->h_red, 64 * sizeof(double)));
+  A3D_CUDA(cudaMalloc(&s->d_flag, 16));
+  A3D_CUDA(cudaMalloc(&s->prevR, N * sizeof(float)));
+  A3D_TRY(build_force_list(s));
+  const double F0[5] = {1, 0, 0, 0, 1 / (kGamma * (kGamma - 1))};  // src/air_cfd.js:162
+  for (int c = 0; c < 5; c++) { s->F[c] = F0[c]; s->fix[0][c] = s->fix[1][c] = s->fix[2][c] = F0[c]; }
+  A3D_CUDA(cudaStreamSynchronize(s->st));
+  return A3D_OK;
+}
+
+}  // namespace a3d
+
+using namespace a3d;
+
+namespace {
+
+int new_solver(int device, const int32_t dims[3], const double* xf, const double* yf, const double* zf,
+               a3d_solver** out) {
+  A3D_ARG(out && dims && xf && yf && zf, "null pointer");
+  A3D_ARG(dims[0] >= 1 && dims[1] >= 2 && dims[2] >= 1, "grid dims (NY >= 2 for the symmetry mirror)");
+  A3D_ARG((double)dims[0] * dims[1] * dims[2] < 2.0e9, "grid too large");
+  A3D_TRY(use_device(device));
+  a3d_solver* s = new a3d_solver();
+  cudaGetDevice(&s->device);
+  if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) {
+    delete s;
+    set_error("cudaStreamCreate failed");
+    return A3D_ERR_CUDA;
+  }
+  s->N = (long)dims[0] * dims[1] * dims[2];
+  int rc = grid_upload(dims, xf, yf, zf, s->st, s->grid);
+  if (rc == A3D_OK) rc = geom_alloc(s->N, s->geo);
+  if (rc != A3D_OK) { a3d_solver_destroy(s); return rc; }
+  *out = s;
+  return A3D_OK;
+}
+
+}  // namespace
+
+extern "C" int a3d_solver_create(const int32_t dims[3], const double* xf, const double* yf, const double* zf,
+                                 const uint8_t* t, const float* phi, const float* ap0, const float* ap1,
+                                 const float* ap2, const float* ap3, int device, a3d_solver** out) {
+  clear_error();
+  A3D_ARG(t && phi && ap0 && ap1 && ap2 && ap3, "null geometry array");
+  a3d_solver* s = nullptr;
+  A3D_TRY(new_solver(device, dims, xf, yf, zf, &s));
+  const long N = s->N;
+  int rc = A3D_OK;
+  cudaError_t e = cudaMemcpy(s->geo.t, t, N, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(s->geo.phi, phi, N * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(s->geo.ap0, ap0, N * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(s->geo.ap1, ap1, N * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(s->geo.ap2, ap2, N * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(s->geo.ap3, ap3, N * 4, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) { set_error("geometry upload: %s", cudaGetErrorString(e)); rc = A3D_ERR_CUDA; }
+  if (rc == A3D_OK) rc = solver_finish_setup(s);
+  if (rc != A3D_OK) { a3d_solver_destroy(s); return rc; }
+  *out = s;
+  return A3D_OK;
+}
+
+extern "C" int a3d_solver_create_shape(const a3d_shape* shape, const int32_t dims[3], const double* xf,
+                                       const double* yf, const double* zf, double h, double delta_deg, int device,
+                                       a3d_solver** out) {
+  clear_error();
+  A3D_ARG(shape, "null shape");
+  a3d_solver* s = nullptr;
+  A3D_TRY(new_solver(device, dims, xf, yf, zf, &s));
+  int rc = geom_build_device(*shape, s->grid, h, delta_deg, s->geo, s->st, nullptr, nullptr);
+  if (rc == A3D_OK) rc = solver_finish_setup(s);
+  if (rc != A3D_OK) { a3d_solver_destroy(s); return rc; }
+  *out = s;
+  return A3D_OK;
+}
+
+extern "C" int a3d_solver_destroy(a3d_solver* s) {
+  if (!s) return A3D_OK;
+  cudaSetDevice(s->device);
+  if (s->st) cudaStreamSynchronize(s->st);
+  cudaFree(s->state);
+  cudaFree(s->code);
+  cudaFree(s->d_red);
+  if (s->h_red) cudaFreeHost(s->h_red);
+  cudaFree(s->d_flag);
+  cudaFree(s->prevR);
+  if (s->fl.block) cudaFree(s->fl.block);
+  geom_free(s->geo);
+  grid_free(s->grid);
+  if (s->st) cudaStreamDestroy(s->st);
+  delete s;
+  return A3D_OK;
+}
+
+extern "C" int a3d_solver_dims(a3d_solver* s, int32_t dims[3], int64_t* n_cells) {
+  clear_error();
+  A3D_ARG(s, "null solver");
+  if (dims) { dims[0] = s->grid.NX; dims[1] = s->grid.NY; dims[2] = s->grid.NZ; }
+  if (n_cells) *n_cells = s->N;
+  return A3D_OK;
+}
+
+extern "C" int a3d_solver_set_opt(a3d_solver* s, double cfl, int32_t order) {
+  clear_error();
+  A3D_ARG(s, "null solver");
+  A3D_ARG(cfl > 0 && cfl < 10, "cfl");
+  A3D_ARG(order == 1 || order == 2, "order must be 1 or 2");
+  s->cfl = cfl;
+  s->order = order;
+  return A3D_OK;
+}
+
+extern "C" int a3d_solver_set_free(a3d_solver* s, const double F[5]) {
+  clear_error();
+  A3D_ARG(s && F, "null pointer");
+  for (int c = 0; c < 5; c++) s->F[c] = F[c];
+  return A3D_OK;
+}
+
+extern "C" int a3d_solver_set_fix(a3d_solver* s, const double fix[15]) {
+  clear_error();
+  A3D_ARG(s && fix, "null pointer");
+  for (int c = 0; c < 15; c++) s->fix[c / 5][c % 5] = fix[c];
+  return A3D_OK;
+}
+
+extern "C" int a3d_solver_reset(a3d_solver* s) {
+  clear_error();
+  A3D_ARG(s, "null solver");
+  A3D_CUDA(cudaSetDevice(s->device));
+  k_fill<<<blocks_for(s->N), 256, 0, s->st>>>(s->buf[s->iQ], s->Np, s->N, (float)s->F[0], (float)s->F[1],
+                                               (float)s->F[2], (float)s->F[3], (float)s->F[4]);
+  A3D_CUDA(cudaGetLastError());
+  s->it = 0;
+  s->havePrev = false;
+  s->prevIt = 0;
+  return A3D_OK;
+}
+
+extern "C" int a3d_solver_step(a3d_solver* s, int32_t n) {
+  clear_error();
+  A3D_ARG(s, "null solver");
+  A3D_ARG(n >= 0, "negative iteration count");
+  A3D_CUDA(cudaSetDevice(s->device));
+  StageArgs a1, a2;
+  for (int i = 0; i < n; i++) {
+    float *Q = s->buf[s->iQ], *S1 = s->buf[s->iS1], *B = s->buf[s->iB];
+    fill_stage_args(s, a1, Q, Q, S1, 0.f, 1.f);
+    A3D_TRY(launch_stage(s, a1));
+    fill_stage_args(s, a2, S1, Q, B, 0.5f, 0.5f);
+    A3D_TRY(launch_stage(s, a2));
+    std::swap(s->iQ, s->iB);
+    s->it++;
+  }
+  return A3D_OK;
+}
+
+extern "C" int a3d_solver_iterations(a3d_solver* s, int64_t* it) {
+  clear_error();
+  A3D_ARG(s && it, "null pointer");
+  *it = s->it;
+  return A3D_OK;
+}
+
+extern "C" int a3d_solver_read(a3d_solver* s, float* r, float* ru, float* rv, float* rw, float* E) {
+  clear_error();
+  A3D_ARG(s && r && ru && rv && rw && E, "null pointer");
+  A3D_CUDA(cudaSetDevice(s->device));
+  float* dst[5] = {r, ru, rv, rw, E};
+  const float* Q = s->buf[s->iQ];
+  for (int c = 0; c < 5; c++)
+    A3D_CUDA(cudaMemcpyAsync(dst[c], Q + c * s->Np, s->N * sizeof(float), cudaMemcpyDeviceToHost, s->st));
+  A3D_CUDA(cudaStreamSynchronize(s->st));
+  return A3D_OK;
+}
+
+extern "C" int a3d_solver_write(a3d_solver* s, const float* r, const float* ru, const float* rv, const float* rw,
+                                const float* E) {
+  clear_error();
+  A3D_ARG(s && r && ru && rv && rw && E, "null pointer");
+  A3D_CUDA(cudaSetDevice(s->device));
+  const float* src[5] = {r, ru, rv, rw, E};
+  float* Q = s->buf[s->iQ];
+  for (int c = 0; c < 5; c++)
+    A3D_CUDA(cudaMemcpyAsync(Q + c * s->Np, src[c], s->N * sizeof(float), cudaMemcpyHostToDevice, s->st));
+  A3D_CUDA(cudaStreamSynchronize(s->st));
+  return A3D_OK;
+}
+
+// Selects the stage kernel (0: per-cell, 1: z-march) and the march's z planes per CTA.
+// Not part of the reference surface; used by the parity tests and the autotuner.
+extern "C" int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t march_kz) {
+  clear_error();
+  A3D_ARG(s, "null solver");
+  A3D_ARG(kernel == KERNEL_CELL || kernel == KERNEL_MARCH, "kernel");
+  A3D_ARG(march_kz >= 1 && march_kz <= 1024, "march_kz");
+  s->kernel = kernel;
+  s->march_kz = march_kz;
+  return A3D_OK;
+}
+
+extern "C" int a3d_solver_stream(a3d_solver* s, void** stream) {
+  clear_error();
+  A3D_ARG(s && stream, "null pointer");
+  *stream = (void*)s->st;
+  return A3D_OK;
+}
+
+extern "C" int a3d_solver_sync(a3d_solver* s) {
+  clear_error();
+  A3D_ARG(s, "null solver");
+  A3D_CUDA(cudaSetDevice(s->device));
+  A3D_CUDA(cudaStreamSynchronize(s->st));
+  return A3D_OK;
+}

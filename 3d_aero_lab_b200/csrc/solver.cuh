@@ -1,0 +1,74 @@
+// solver.cuh - one solver case: device state, geometry codes, force list, reduction scratch.
+#pragma once
+#include "geom.cuh"
+
+namespace a3d {
+
+// Arguments of one RK stage (src/air_cfd.js:237-251): Out = wa*B + wb*(Qin + dt*R(Qin)).
+struct StageArgs {
+  const float* __restrict__ Qin;
+  const float* __restrict__ B;
+  float* __restrict__ Out;
+  long Np;                       // component stride of the SoA state (5 components)
+  const uint8_t* __restrict__ code;
+  const float* __restrict__ phi;
+  const float* __restrict__ ap0;
+  const float* __restrict__ ap1;
+  const float* __restrict__ ap2;
+  const float* __restrict__ ap3;
+  const float* __restrict__ rXd;  // 1/dx, 1/dy, 1/dz (float32)
+  const float* __restrict__ rYd;
+  const float* __restrict__ rZd;
+  int NX, NY, NZ;
+  float wa, wb, cfl;
+  int order2;                     // 1: MUSCL-minmod, 0: first order (opt.order)
+  float Pff[5];                   // primitive far-field state (rho, u, v, w, p)
+  float Pfix[3][5];               // primitive fixed states of types 3, 4, 5
+  float Ufix[3][5];               // conservative fixed states written to fixed cells
+};
+
+// Device-side force-list entry arrays (cfdForceList).
+struct ForceList {
+  long n = 0;
+  int64_t* q = nullptr;
+  double *cx = nullptr, *cz = nullptr, *x = nullptr, *z = nullptr;
+  void* block = nullptr;
+};
+
+enum StageKernel { KERNEL_CELL = 0, KERNEL_MARCH = 1 };
+
+}  // namespace a3d
+
+struct a3d_solver {
+  int device = 0;
+  cudaStream_t st = nullptr;
+  a3d::GridDev grid;
+  a3d::GeomDev geo;
+  long N = 0, Np = 0;
+  float* state = nullptr;         // 3 buffers x 5 components x Np floats
+  float* buf[3] = {nullptr, nullptr, nullptr};
+  int iQ = 0, iS1 = 1, iB = 2;
+  uint8_t* code = nullptr;
+  a3d::ForceList fl;
+  double F[5];
+  double fix[3][5];
+  double cfl = 0.7;
+  int order = 2;
+  long it = 0;
+  int kernel = a3d::KERNEL_MARCH;
+  int march_kz = 16;              // z planes per CTA of the march kernel
+  // reductions
+  double* d_red = nullptr;        // device partials + results
+  double* h_red = nullptr;        // pinned host mirror of the results
+  int* d_flag = nullptr;          // non-finite flag
+  float* prevR = nullptr;         // density snapshot for the residual
+  long prevIt = 0;
+  bool havePrev = false;
+};
+
+namespace a3d {
+int solver_finish_setup(a3d_solver* s);           // codes + force list + state buffers
+int launch_stage(a3d_solver* s, const StageArgs& a);
+void fill_stage_args(a3d_solver* s, StageArgs& a, const float* Qin, const float* B, float* Out, float wa, float wb);
+int build_force_list(a3d_solver* s);
+}  // namespace a3d

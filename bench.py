@@ -1,0 +1,304 @@
+"""Benchmark of the plain 3D Euler cut-cell solve on B200 (one JSON line on rank 0).
+
+Workload (the largest single-GPU plain configuration the metric is quoted on): the fighter
+half model at ~4M cells (stretched grid ~200 x 140 x 140), M0.6, alpha 3 deg, delta 3 deg,
+free-stream fixed states, SSP-RK2 with cfl 0.7, MUSCL order 2.  One *step* is one solve:
+reset + ITERS iterations + the FP64 force integral.  Inputs are synthetic in the sense that
+the reference publishes no dataset; the geometry is the reference's own parametric fighter.
+
+value  - cell-updates/s with the state resident in HBM (CUDA events on the solver stream);
+e2e    - the same through the public solver API with host buffers: each step uploads the
+         initial state from pinned memory, solves, reads the full state back and computes
+         the forces (CUDA events around the whole sequence on the solver stream).
+roofline.achieved - 142 algorithmic bytes per cell-update (stage 1: read Q + metadata 41 B,
+         write S1 20 B; stage 2: read S1, Q and metadata 61 B, write B 20 B) x cell-updates/s.
+
+--impl reference times the reference's CPU algorithm instead (the C++ restatement of CfdCPU,
+OpenMP over all host cores): the JavaScript original cannot run on this machine.
+Multi-GPU (torchrun): each rank solves its own case (weak scaling); timings are the max
+over ranks.
+"""
+import argparse
+import importlib
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ALG_BYTES_PER_CELL_UPDATE = 142
+WORKLOAD = {"aircraft": "fighter", "cells": 4.0e6, "M": 0.6, "alpha": 3.0, "delta": 3.0, "iters": 2000}
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--iters", type=int, default=WORKLOAD["iters"])
+    p.add_argument("--cells", type=float, default=WORKLOAD["cells"])
+    p.add_argument("--kernel", type=int, default=1)
+    p.add_argument("--kz", type=int, default=16)
+    p.add_argument("--cpu-sample-iters", type=int, default=2)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region (clocks and throttle reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.p = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+
+    def start(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if not self.p:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        load = [v for v in sm if smax and v > 0.3 * smax] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        backend = "nccl" if (args.impl == "ours" and torch.cuda.is_available()) else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=timedelta(seconds=300))
+    return ws, rank, local
+
+
+def max_over_ranks(v, ws):
+    if ws == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([v], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def cpu_baseline(aero, sh, cells, iters, threads):
+    """The oracle (C++ CfdCPU restatement, f32 storage / f64 arithmetic) on a bounded sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref
+    g = ref.grid(sh, cells)
+    geo = ref.geom(sh, g, WORKLOAD["delta"])
+    s = ref.CfdCPU(g, geo, threads=threads)
+    F = aero.cfd.freestream(WORKLOAD["M"], WORKLOAD["alpha"])
+    s.setFree(F)
+    s.setFix([F, F, F])
+    s.reset()
+    s.step(1)  # untimed warm-up iteration
+    t0 = time.perf_counter()
+    s.step(iters)
+    dt = time.perf_counter() - t0
+    return g.N * iters / dt, g.N
+
+
+def run_reference(args, ws, rank):
+    """--impl reference: the reference's CPU algorithm (oracle port, all host threads)."""
+    if rank != 0:
+        return
+    aero = importlib.import_module("3d_aero_lab_b200")
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref
+    threads = ref.max_threads()
+    sh = aero.shape_of(aero.build_aircraft(WORKLOAD["aircraft"]))
+    g = ref.grid(sh, args.cells)
+    geo = ref.geom(sh, g, WORKLOAD["delta"])
+    s = ref.CfdCPU(g, geo, threads=threads)
+    F = aero.cfd.freestream(WORKLOAD["M"], WORKLOAD["alpha"])
+    s.setFree(F)
+    s.setFix([F, F, F])
+    s.reset()
+    per_step = max(1, args.cpu_sample_iters)
+    for _ in range(args.warmup):
+        s.step(1)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        s.step(per_step)
+    dt = time.perf_counter() - t0
+    v = g.N * per_step * args.steps / dt
+    sample = f"{per_step} iterations per step of the {g.NX}x{g.NY}x{g.NZ} fighter grid"
+    out = {"metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+           "impl": "reference",
+           "config": {"workload": "fighter plain solve, CPU reference algorithm (C++ CfdCPU restatement)",
+                      "cells": g.N, "dims": [g.NX, g.NY, g.NZ]},
+           "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port", "sample": sample},
+           "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        return
+    import numpy as np
+    import torch
+    aero = importlib.import_module("3d_aero_lab_b200")
+    torch.cuda.set_device(local)
+    alpha = WORKLOAD["alpha"] + 0.25 * rank  # independent case per rank
+    ac = aero.build_aircraft(WORKLOAD["aircraft"])
+    sh = aero.shape_of(ac)
+    case = aero.Case(ac=ac, cells=args.cells, M=WORKLOAD["M"], alpha=alpha, delta=WORKLOAD["delta"], device=local)
+    s = case.solver
+    s.set_kernel(args.kernel, args.kz)
+    g = case.g
+    N = g.N
+    stream = torch.cuda.ExternalStream(s.stream, device=torch.device("cuda", local))
+    iters = args.iters
+    launches_per_step = 1 + 2 * iters + 2  # reset fill, two stages per iteration, force reduction
+
+    def solve():
+        s.reset()
+        s.step(iters)
+        return case.forces()
+
+    for _ in range(args.warmup):
+        solve()
+    s.sync()
+    # ---- device-resident timing ----
+    clk = Clocks(local)
+    barrier(ws)
+    torch.cuda.synchronize()
+    clk.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        f = solve()
+    e1.record(stream)
+    e1.synchronize()
+    clocks = clk.stop()
+    ms = e0.elapsed_time(e1) / args.steps
+    ms = max_over_ranks(ms, ws)
+    barrier(ws)
+    # ---- stage-kernel time alone (dominant kernel) ----
+    k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.reset()
+    k0.record(stream)
+    s.step(iters)
+    k1.record(stream)
+    k1.synchronize()
+    stage_ms = k0.elapsed_time(k1) / (2 * iters)
+    # ---- end to end through the public API with pinned host buffers ----
+    Q0 = torch.empty((5, N), dtype=torch.float32, pin_memory=True)
+    Q0.numpy()[:] = np.asarray(case.F, np.float32)[:, None]
+    Hout = {k: torch.empty(N, dtype=torch.float32, pin_memory=True) for k in ("r", "ru", "rv", "rw", "E")}
+    Hnp = {k: v.numpy() for k, v in Hout.items()}
+    barrier(ws)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    for _ in range(args.steps):
+        s.write(Q0.numpy())
+        s.step(iters)
+        s.read(Hnp)
+        fe = case.forces()
+    t1.record(stream)
+    t1.synchronize()
+    e2e_ms = max_over_ranks(t0.elapsed_time(t1) / args.steps, ws)
+    cu = N * iters
+    value = ws * cu / (ms * 1e-3)
+    e2e = ws * cu / (e2e_ms * 1e-3)
+    peak, peak_kind = peaks()
+    achieved = ALG_BYTES_PER_CELL_UPDATE / 2 * N / (stage_ms * 1e-3) / 1e9
+    out = None
+    if rank == 0:
+        cpu = None
+        if not args.no_cpu_baseline and ws == 1:
+            v, n_cpu = cpu_baseline(aero, sh, args.cells, args.cpu_sample_iters, 1)
+            cpu = {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": "port",
+                   "sample": f"{args.cpu_sample_iters} iterations of the same {g.NX}x{g.NY}x{g.NZ} grid, 1 thread "
+                             "(C++ restatement of CfdCPU; the JavaScript original cannot run here)"}
+        out = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": ws,
+               "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+               "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+               "config": {"workload": f"fighter plain solve, {g.NX}x{g.NY}x{g.NZ} = {N} cells, M0.6 a3 d3, "
+                                      f"{iters} SSP-RK2 iterations per step",
+                          "cells": N, "dims": [g.NX, g.NY, g.NZ], "iterations_per_step": iters,
+                          "kernel": "march" if args.kernel == 1 else "cell", "march_kz": args.kz,
+                          "l2": "inputs larger than L2 (three 5-component float32 states of %.0f MB each)"
+                                % (20 * N / 1e6),
+                          "parallelism": f"{ws} independent solves (one per GPU)" if ws > 1 else "single GPU"},
+               "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": 20 * N,
+                       "d2h_bytes_per_step": 20 * N + 24},
+               "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                            "frac": achieved / peak, "traffic": None,
+                            "peak_source": peak_kind, "kernel": "k_stage_march" if args.kernel == 1 else "k_stage_cell",
+                            "stage_ms": stage_ms},
+               "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches_per_step * args.steps,
+               "forces": {"CL": f["CL"], "CD": f["CD"], "Cm": f["Cm"], "CL_e2e": fe["CL"]}}
+        print(json.dumps(out), flush=True)
+    s.dispose()
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -160,6 +160,15 @@ int a3d_solver_trefftz(a3d_solver* s, double xT, double alpha_deg, double M, dou
 int a3d_solver_residual(a3d_solver* s, int32_t stride, double* res);
 /* Largest Mach number over fluid cells with q % stride == 0 (src/air_cfd.js:571). */
 int a3d_solver_mach_max(a3d_solver* s, int32_t stride, double* mmax);
+/* Stage kernel selection; no counterpart in the reference (it has one shader).
+ * kernel 0: one thread per cell evaluating its six faces (the reference's structure);
+ * kernel 1 (default): z-marching tiles that evaluate every face once; march_kz = z planes
+ * per thread block.                                                                   */
+int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t march_kz);
+/* The solver's CUDA stream (a cudaStream_t), for callers that time or order work on it. */
+int a3d_solver_stream(a3d_solver* s, void** stream);
+/* Blocks until all work queued on the solver's stream has finished. */
+int a3d_solver_sync(a3d_solver* s);
 
 #ifdef __cplusplus
 }

@@ -696,3 +696,6 @@ int ref_max_threads(void) {
 }
 
 }  // extern "C"
+
+extern "C" void ref_hllc(const double* L, const double* R, int d, double* out) { cfdHLLC(L, R, d, out); }
+extern "C" void ref_prim(const double* U, double* P) { cfdPrim5(U[0], U[1], U[2], U[3], U[4], P); }

@@ -63,7 +63,7 @@ def lib():
 class Grid:
     """cfdGrid output: face coordinates (f64) plus the float32 centres/sizes the reference keeps."""
 
-    def __init__(self, xf, yf, zf, h, core):
+    def __init__(self, xf, yf, zf, h=1.0, core=None):
         self.xf, self.yf, self.zf, self.h, self.core = xf, yf, zf, h, core
         self.dims = np.array([len(xf) - 1, len(yf) - 1, len(zf) - 1], dtype=np.int32)
         self.NX, self.NY, self.NZ = (int(v) for v in self.dims)
@@ -175,3 +175,22 @@ class CfdCPU:
 
 def max_threads():
     return lib().ref_max_threads()
+
+
+def hllc(L, R, d):
+    """HLLC flux of the oracle (cfdHLLC) for primitive states L, R along direction d."""
+    lb = lib()
+    lb.ref_hllc.argtypes = [_dp, _dp, C.c_int, _dp]
+    lb.ref_hllc.restype = None
+    out = np.zeros(5)
+    lb.ref_hllc(np.asarray(L, np.float64), np.asarray(R, np.float64), int(d), out)
+    return out
+
+
+def prim(U):
+    lb = lib()
+    lb.ref_prim.argtypes = [_dp, _dp]
+    lb.ref_prim.restype = None
+    out = np.zeros(5)
+    lb.ref_prim(np.asarray(U, np.float64), out)
+    return out

@@ -1,0 +1,137 @@
+"""GPU solver vs the CPU oracle (CfdCPU restatement): state, forces and post-processing.
+
+Tolerances: the GPU computes in float32 like the reference's WebGL shader, the oracle in
+float64 like the reference's JavaScript CPU path; both store float32.  The metric is the
+reference's GPU/CPU one, max|gpu - cpu| / max|cpu| per variable (tools/gpucmp.mjs:19-21),
+bounded by 3e-6 after the README case's 200 iterations; C_L and C_D must agree to 4
+significant digits.  Post-processing reductions are FP64 on both sides: 1e-9 relative.
+"""
+import math
+
+import numpy as np
+import pytest
+
+from helpers import BoxGrid, README_CD, README_CL, box_geometry, freestream, oracle_case, rel_max_diff
+
+pytestmark = pytest.mark.gpu
+
+TOL_STATE = 3e-6
+
+
+def gpu_case(aero, sh, cells, delta, M=0.6, alpha=3.0, kernel=1, fix=None):
+    g = aero.cfd_grid(sh, cells)
+    s = aero.CfdGPU(g, shape=sh, delta=delta)
+    s.set_kernel(kernel)
+    F = freestream(M, alpha)
+    s.setFree(F)
+    s.setFix(fix if fix is not None else [F, F, F])
+    s.reset()
+    return g, s
+
+
+def sig4(x):
+    return float(f"{x:.4g}")
+
+
+@pytest.mark.parametrize("kernel", [0, 1])
+def test_readme_case_matches_oracle_and_pin(aero, ref, kernel):
+    ac, sh, og, ogeo, o = oracle_case(aero, ref, "fighter", 30000, 3.0)
+    g, s = gpu_case(aero, sh, 30000, 3.0, kernel=kernel)
+    o.step(200)
+    s.step(200)
+    Qo, Qg = o.read(), s.read_array()
+    errs = [rel_max_diff(Qg[c], Qo[c]) for c in range(5)]
+    assert max(errs) <= TOL_STATE, errs
+    r = ac.ref
+    fg = s.forces(3.0, 0.6, r["S"], r["xcg"], 0.0, r["c"])
+    fo = o.forces(3.0, 0.6, r["S"], r["xcg"], 0.0, r["c"])
+    assert sig4(fg["CL"]) == sig4(fo["CL"]) and sig4(fg["CD"]) == sig4(fo["CD"])
+    assert round(fg["CL"], 4) == README_CL and round(fg["CD"], 5) == README_CD
+
+
+def test_kernels_agree(aero):
+    sh = aero.shape_of(aero.build_aircraft("airliner"))
+    _, a = gpu_case(aero, sh, 120000, 2.0, M=0.78, alpha=2.5, kernel=0)
+    _, b = gpu_case(aero, sh, 120000, 2.0, M=0.78, alpha=2.5, kernel=1)
+    a.step(60)
+    b.step(60)
+    A, B = a.read_array(), b.read_array()
+    assert max(rel_max_diff(A[c], B[c]) for c in range(5)) < 1e-5
+
+
+@pytest.mark.parametrize("seed,dims,order", [(0, (9, 7, 6), 2), (1, (33, 9, 20), 2), (2, (40, 17, 3), 1),
+                                             (3, (5, 2, 35), 2), (4, (64, 12, 18), 2)])
+@pytest.mark.parametrize("kernel", [0, 1])
+def test_random_boxes_per_cell(aero, ref, seed, dims, order, kernel):
+    """Random cut cells, solids, fixed cells and baffles; every cell after 1 and 15 iterations."""
+    rng = np.random.default_rng(seed)
+    NX, NY, NZ = dims
+    bg = BoxGrid(rng, NX, NY, NZ)
+    t, phi, ap = box_geometry(rng, NX, NY, NZ)
+    geo = ref.Geom()
+    geo.t, geo.phi, geo.ap = t, phi, ap
+    o = ref.CfdCPU(bg, geo)
+    g = aero.cfd.Grid(bg.xf, bg.yf, bg.zf)
+    hgeo = aero.cfd.Geom(bg.N)
+    hgeo.t, hgeo.phi, hgeo.ap = t, phi, ap
+    s = aero.CfdGPU(g, hgeo)
+    s.set_kernel(kernel, 4)
+    F = freestream(0.7, 4.0)
+    fix = [[1.1, 0.3, 0.0, 0.0, 2.1], [0.9, 0.8, 0.05, 0.0, 2.4], [0.7, 1.2, 0.0, -0.1, 3.0]]
+    for x in (o, s):
+        x.setFree(F)
+        x.setFix(fix)
+        x.set_opt(cfl=0.6, order=order)
+        x.reset()
+    # perturb the state so every face sees different left/right states
+    Q0 = o.read()
+    Q0 = Q0 * (1 + 0.05 * rng.standard_normal(Q0.shape))
+    Q0 = Q0.astype(np.float32).astype(np.float64)
+    o.write(Q0)
+    s.write(Q0.astype(np.float32))
+    for n in (1, 14):
+        o.step(n)
+        s.step(n)
+        Qo, Qg = o.read(), s.read_array()
+        for c in range(5):
+            d = np.abs(Qg[c] - Qo[c]) / np.maximum(np.abs(Qo[c]), 1e-3 * np.max(np.abs(Qo[c])))
+            assert np.max(d) < (2e-5 if n == 1 else 3e-4), (c, n, float(np.max(d)))
+
+
+def test_postprocessing_matches_oracle(aero, ref):
+    ac, sh, og, ogeo, o = oracle_case(aero, ref, "airliner", 150000, 1.0, M=0.78, alpha=2.5)
+    g, s = gpu_case(aero, sh, 150000, 1.0, M=0.78, alpha=2.5)
+    o.step(30)
+    Q = o.read()
+    s.write(Q.astype(np.float32))
+    r = ac.ref
+    fo = o.forces(2.5, 0.78, r["S"], r["xcg"], 0.0, r["c"])
+    fg = s.forces(2.5, 0.78, r["S"], r["xcg"], 0.0, r["c"])
+    for k in ("CL", "CD", "Cm"):
+        assert math.isclose(fg[k], fo[k], rel_tol=1e-9, abs_tol=1e-12), k
+    xT = aero.trefftz_x(ac)
+    assert math.isclose(s.trefftz(xT, 2.5, 0.78, r["S"]), o.trefftz(xT, 2.5, 0.78, r["S"]), rel_tol=1e-9)
+    assert math.isclose(s.mach_max(2), o.mach_max(2), rel_tol=1e-12)
+    # residual: snapshot at Q, seven iterations, then compare RMS(Q2 - Q) / 7 on the same states
+    assert s.residual(3) is None and o.residual(3) < 0
+    o.step(7)
+    Q2 = o.read()
+    s.step(7)  # advances the iteration counter; the state is then overwritten with the oracle's
+    s.write(Q2.astype(np.float32))
+    assert math.isclose(s.residual(3), o.residual(3), rel_tol=1e-9)
+
+
+def test_nonfinite_state_is_reported(aero):
+    sh = aero.shape_of(aero.build_aircraft("fighter"))
+    g, s = gpu_case(aero, sh, 8000, 0.0)
+    s.residual(3)
+    s.step(2)
+    Q = s.read_array()
+    fluid = np.nonzero(aero.cfd_geom(sh, g, 0.0).t == 0)[0]
+    Q[0, fluid[fluid % 3 == 0][0]] = np.nan
+    s.write(Q)
+    from importlib import import_module
+    L = import_module("3d_aero_lab_b200._lib")
+    with pytest.raises(L.AeroError) as e:
+        s.residual(3)
+    assert e.value.status == 4

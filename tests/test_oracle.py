@@ -1,0 +1,96 @@
+"""CPU oracle: pinned to the reference's published numbers and to physics known answers."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from helpers import README_CD, README_CL, freestream, oracle_case
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def test_readme_pin_fighter_30k(aero, ref):
+    """README.md:98 - fighter, 30k cells, M0.6, alpha 3, delta 3, 200 iterations: CL 0.1927, CD 0.04406."""
+    ac, sh, g, geo, s = oracle_case(aero, ref, "fighter", 30000, 3.0)
+    s.step(200)
+    f = s.forces(3.0, 0.6, ac.ref["S"], ac.ref["xcg"], 0.0, ac.ref["c"])
+    assert round(f["CL"], 4) == README_CL
+    assert round(f["CD"], 5) == README_CD
+
+
+def test_golden_history_matches_oracle(aero, ref):
+    """Regression of the oracle's own force history against the committed fixture."""
+    gold = json.load(open(os.path.join(GOLDEN, "oracle_fighter30k.json")))
+    ac, sh, g, geo, s = oracle_case(aero, ref, "fighter", gold["cells"], gold["delta"])
+    assert [g.NX, g.NY, g.NZ] == gold["dims"]
+    assert geo.nSolid == gold["nSolid"] and geo.nCut == gold["nCut"]
+    for row in gold["history"]:
+        s.step(row["it"] - s.it)
+        f = s.forces(3.0, 0.6, ac.ref["S"], ac.ref["xcg"], 0.0, ac.ref["c"])
+        assert abs(f["CL"] - row["CL"]) < 1e-12 and abs(f["CD"] - row["CD"]) < 1e-12
+
+
+def test_hllc_consistency(ref):
+    """HLLC(U, U) equals the exact Euler flux of U in every direction."""
+    rng = np.random.default_rng(1)
+    for _ in range(50):
+        P = np.array([rng.uniform(0.2, 2), rng.uniform(-2, 2), rng.uniform(-2, 2), rng.uniform(-2, 2), rng.uniform(0.1, 2)])
+        for d in range(3):
+            F = ref.hllc(P, P, d)
+            r, u, p = P[0], P[1:4], P[4]
+            E = p / 0.4 + 0.5 * r * (u @ u)
+            exact = np.array([r * u[d], r * u[0] * u[d], r * u[1] * u[d], r * u[2] * u[d], u[d] * (E + p)])
+            exact[1 + d] += p
+            assert np.allclose(F, exact, rtol=1e-12, atol=1e-12)
+
+
+def test_uniform_freestream_is_fixed_point(ref):
+    """An empty box with a float32-exact free stream stays exactly uniform (src/air_cfd.js:205-249)."""
+    NX, NY, NZ = 7, 5, 6
+    N = NX * NY * NZ
+    g = ref.Grid(np.linspace(0, 7, NX + 1), np.linspace(0, 5, NY + 1) ** 1.2, np.linspace(-3, 3, NZ + 1))
+    geo = ref.Geom()
+    geo.t = np.zeros(N, np.uint8)
+    geo.phi = np.ones(N, np.float32)
+    geo.ap = [np.ones(N, np.float32)] * 3 + [np.zeros(N, np.float32)]
+    s = ref.CfdCPU(g, geo)
+    F = [1.0, 0.5, 0.0, 0.25, 2.0]
+    s.setFree(F)
+    s.setFix([F, F, F])
+    s.reset()
+    s.step(5)
+    Q = s.read()
+    for c in range(5):
+        assert np.all(Q[c] == np.float32(F[c]))
+
+
+def test_symmetric_inputs_give_symmetric_fp64_and_fp32(aero, ref):
+    """FP32-storage and FP64-storage runs of the same scheme stay close (error vs FP64 is small)."""
+    ac, sh, g, geo, s32 = oracle_case(aero, ref, "fighter", 8000, 0.0, prec=32)
+    _, _, _, _, s64 = oracle_case(aero, ref, "fighter", 8000, 0.0, prec=64)
+    s32.step(40)
+    s64.step(40)
+    a, b = s32.read(), s64.read()
+    for c in range(5):
+        assert np.max(np.abs(a[c] - b[c])) / np.max(np.abs(b[c])) < 1e-4
+
+
+def test_thread_count_does_not_change_results(aero, ref):
+    ac, sh, g, geo, s1 = oracle_case(aero, ref, "fighter", 6000, 3.0, threads=1)
+    _, _, _, _, s8 = oracle_case(aero, ref, "fighter", 6000, 3.0, threads=8)
+    s1.step(10)
+    s8.step(10)
+    assert np.array_equal(s1.read(), s8.read())
+
+
+@pytest.mark.parametrize("typ", ["airliner", "interceptor"])
+def test_other_types_build_and_step(aero, ref, typ):
+    ac, sh, g, geo, s = oracle_case(aero, ref, typ, 12000, 2.0, M=0.7, alpha=2.0)
+    assert geo.nSolid > 0 and geo.nCut > 0
+    s.step(20)
+    Q = s.read()
+    assert np.all(np.isfinite(Q)) and np.all(Q[0] > 0)
+    if typ == "airliner":
+        assert np.count_nonzero(geo.t == 3) > 0 and np.count_nonzero(geo.t == 4) > 0
+    assert np.count_nonzero(geo.t == 5) > 0
