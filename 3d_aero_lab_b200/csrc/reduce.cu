@@ -102,9 +102,11 @@ __global__ void k_finalize(const double* partials, double* out) {
 }
 
 struct PostArgs {
-  const float* Q;  // current state, component stride Np
+  const float* Q;  // current state, component stride Np, row pitch NXp
   long Np, N;
-  const uint8_t* t;
+  int NX, NXp;
+  const uint8_t* t;  // cell types in the reference layout
+  __device__ __forceinline__ long pad(long q) const { return (q / NX) * NXp + q % NX; }
 };
 
 __global__ void k_forces(PostArgs p, long n, const int64_t* fq, const double* fcx, const double* fcz,
@@ -112,7 +114,7 @@ __global__ void k_forces(PostArgs p, long n, const int64_t* fq, const double* fc
   double v[3] = {0, 0, 0};
   const double pinf = 1 / kCG;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x) {
-    const long q = fq[e];
+    const long q = p.pad(fq[e]);
     const double r = p.Q[q], u = (double)p.Q[p.Np + q] / r, vv = (double)p.Q[2 * p.Np + q] / r,
                  w = (double)p.Q[3 * p.Np + q] / r;
     const double dp = (kCG - 1) * ((double)p.Q[4 * p.Np + q] - 0.5 * r * (u * u + vv * vv + w * w)) - pinf;
@@ -130,8 +132,8 @@ __global__ void k_trefftz(PostArgs p, int NX, int NY, int NZ, int i0, double tx,
     const int j = (int)(e % NY), k = (int)(e / NY);
     double u = 0, vv = 0, w = 0, ws = 0;
     for (int di = 0; di < 2; di++) {
-      const long q = ((long)k * NY + j) * NX + i0 + di;
-      if (p.t[q] != T_FLUID) continue;
+      const long qr = ((long)k * NY + j) * NX + i0 + di, q = ((long)k * NY + j) * p.NXp + i0 + di;
+      if (p.t[qr] != T_FLUID) continue;
       const double ww = di ? tx : 1 - tx, r = p.Q[q];
       u += ww * (double)p.Q[p.Np + q] / r;
       vv += ww * (double)p.Q[2 * p.Np + q] / r;
@@ -151,8 +153,8 @@ __global__ void k_residual(PostArgs p, const float* prevR, int stride, double* p
   const long M = (p.N + stride - 1) / stride;
   bool bad = false;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < M; e += (long)gridDim.x * blockDim.x) {
-    const long q = e * stride;
-    if (p.t[q] != T_FLUID) continue;
+    const long qr = e * stride, q = p.pad(qr);
+    if (p.t[qr] != T_FLUID) continue;
     const float r = p.Q[q];
     if (!isfinite(r)) bad = true;
     const double d = (double)r - (double)prevR[q];
@@ -168,8 +170,8 @@ __global__ void k_mach(PostArgs p, int stride, double* partials) {
   double m2max = 0;
   const long M = (p.N + stride - 1) / stride;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < M; e += (long)gridDim.x * blockDim.x) {
-    const long q = e * stride;
-    if (p.t[q] != T_FLUID) continue;
+    const long qr = e * stride, q = p.pad(qr);
+    if (p.t[qr] != T_FLUID) continue;
     const double r = p.Q[q], u = (double)p.Q[p.Np + q] / r, v = (double)p.Q[2 * p.Np + q] / r,
                  w = (double)p.Q[3 * p.Np + q] / r;
     const double pr = (kCG - 1) * ((double)p.Q[4 * p.Np + q] - 0.5 * r * (u * u + v * v + w * w));
@@ -204,6 +206,8 @@ PostArgs post_args(a3d_solver* s) {
   p.Q = s->buf[s->iQ];
   p.Np = s->Np;
   p.N = s->N;
+  p.NX = s->grid.NX;
+  p.NXp = s->NXp;
   p.t = s->geo.t;
   return p;
 }
@@ -353,7 +357,7 @@ extern "C" int a3d_solver_residual(a3d_solver* s, int32_t stride, double* res_ou
     res = std::sqrt(s->h_red[0] / std::max(1.0, s->h_red[1])) / (double)nIt;
     if (flag) { set_error("non-finite density in the state"); rc = A3D_ERR_NONFINITE; }
   }
-  A3D_CUDA(cudaMemcpyAsync(s->prevR, s->buf[s->iQ], s->N * sizeof(float), cudaMemcpyDeviceToDevice, s->st));
+  A3D_CUDA(cudaMemcpyAsync(s->prevR, s->buf[s->iQ], s->Np * sizeof(float), cudaMemcpyDeviceToDevice, s->st));
   A3D_CUDA(cudaStreamSynchronize(s->st));
   s->prevIt = s->it;
   s->havePrev = true;

@@ -1,7 +1,8 @@
 // solver.cu - the SSP-RK2 cut-cell Euler solver object (CfdCPU / CfdGPU, src/air_cfd.js:157-438).
 //
 // State: three structure-of-arrays float32 buffers Q, S1, B (rho, rho*u, rho*v, rho*w, E),
-// each component padded to a multiple of 64 cells.  One iteration is two stage launches:
+// each component a [NZ][NY][NXp] array with the row pitch NXp = NX rounded up to 16 (the
+// alignment TMA tiles need).  One iteration is two stage launches:
 //   S1 = Q + dt R(Q)                         (stage 1, dt from Q)
 //   B  = 0.5 Q + 0.5 (S1 + dt R(S1))         (stage 2, dt again from Q)
 // followed by a buffer rotation Q <-> B (src/air_cfd.js:252-258).  dt is recomputed from
@@ -26,7 +27,7 @@ namespace {
 // ----------------------------------------------------------------------------------------
 // per-cell codes: type, static slope-test bits, irregular and baffle flags
 // ----------------------------------------------------------------------------------------
-__global__ void k_codes(int NX, int NY, int NZ, const uint8_t* t, const float* phi, const float* ap0,
+__global__ void k_codes(int NX, int NY, int NZ, int NXp, const uint8_t* t, const float* phi, const float* ap0,
                         const float* ap1, const float* ap2, const float* ap3, uint8_t* code) {
   const long NXY = (long)NX * NY, N = NXY * NZ;
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < N; q += (long)gridDim.x * blockDim.x) {
@@ -42,12 +43,12 @@ __global__ void k_codes(int NX, int NY, int NZ, const uint8_t* t, const float* p
     }
     if (phi[q] != 1.f || ap0[q] != 1.f || ap1[q] != 1.f || ap2[q] != 1.f) c |= C_IRR;
     if (ap3[q] != 0.f || (k > 0 && ap3[q - NXY] != 0.f)) c |= C_BAF;
-    code[q] = c;
+    code[((long)k * NY + j) * NXp + i] = c;
   }
 }
 
-__global__ void k_fill(float* Q, long Np, long N, float f0, float f1, float f2, float f3, float f4) {
-  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < N; q += (long)gridDim.x * blockDim.x) {
+__global__ void k_fill(float* Q, long Np, float f0, float f1, float f2, float f3, float f4) {
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < Np; q += (long)gridDim.x * blockDim.x) {
     Q[q] = f0; Q[Np + q] = f1; Q[2 * Np + q] = f2; Q[3 * Np + q] = f3; Q[4 * Np + q] = f4;
   }
 }
@@ -66,7 +67,7 @@ __device__ __forceinline__ int stencil_prim(const StageArgs& a, int i, int j, in
   }
   const bool mirror = j < 0;
   const int jj = mirror ? -1 - j : j;
-  const long q = ((long)k * a.NY + jj) * a.NX + i;
+  const long q = ((long)k * a.NY + jj) * a.NXp + i;
   const int t = a.code[q] & 7;
   if (t >= T_SINK) { for (int v = 0; v < 5; v++) P[v] = a.Pfix[t - T_SINK][v]; }
   else cons_to_prim(a.Qin[q], a.Qin[a.Np + q], a.Qin[2 * a.Np + q], a.Qin[3 * a.Np + q], a.Qin[4 * a.Np + q], P);
@@ -79,16 +80,17 @@ __global__ void __launch_bounds__(256) k_stage_cell(StageArgs a) {
   const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (q >= N) return;
   const int i = (int)(q % a.NX), j = (int)((q / a.NX) % a.NY), k = (int)(q / NXY);
-  const uint8_t cq = a.code[q];
+  const long qp = ((long)k * a.NY + j) * a.NXp + i;  // padded state/code index
+  const uint8_t cq = a.code[qp];
   const int t = cq & 7;
   const long Np = a.Np;
   if (t != T_FLUID) {  // src/air_cfd.js:242
-    if (t >= T_SINK) for (int c = 0; c < 5; c++) a.Out[c * Np + q] = a.Ufix[t - T_SINK][c];
-    else for (int c = 0; c < 5; c++) a.Out[c * Np + q] = a.B[c * Np + q];
+    if (t >= T_SINK) for (int c = 0; c < 5; c++) a.Out[c * Np + qp] = a.Ufix[t - T_SINK][c];
+    else for (int c = 0; c < 5; c++) a.Out[c * Np + qp] = a.B[c * Np + qp];
     return;
   }
   float Pc[5];
-  cons_to_prim(a.Qin[q], a.Qin[Np + q], a.Qin[2 * Np + q], a.Qin[3 * Np + q], a.Qin[4 * Np + q], Pc);
+  cons_to_prim(a.Qin[qp], a.Qin[Np + qp], a.Qin[2 * Np + qp], a.Qin[3 * Np + qp], a.Qin[4 * Np + qp], Pc);
   const float pC = Pc[4];
   float R[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
   const float* apd[3] = {a.ap0, a.ap1, a.ap2};
@@ -145,18 +147,18 @@ __global__ void __launch_bounds__(256) k_stage_cell(StageArgs a) {
   // local time step from the base state (src/air_cfd.js:243, CFD3_FS :357-359)
   float Pb[5];
   if (a.wa == 0.f) { for (int v = 0; v < 5; v++) Pb[v] = Pc[v]; }
-  else cons_to_prim(a.B[q], a.B[Np + q], a.B[2 * Np + q], a.B[3 * Np + q], a.B[4 * Np + q], Pb);
+  else cons_to_prim(a.B[qp], a.B[Np + qp], a.B[2 * Np + qp], a.B[3 * Np + qp], a.B[4 * Np + qp], Pb);
   const float as = sqrtf(kG * Pb[4] / Pb[0]);
   const float dt = a.cfl * fmaxf(ph, 0.25f) / ((fabsf(Pb[1]) + as) * rh[0] + (fabsf(Pb[2]) + as) * rh[1] + (fabsf(Pb[3]) + as) * rh[2]);
   float o[5];
   for (int c = 0; c < 5; c++) {
-    const float qin = a.Qin[c * Np + q];
-    o[c] = (a.wa == 0.f) ? (qin + dt * R[c]) : (a.wa * a.B[c * Np + q] + a.wb * (qin + dt * R[c]));
+    const float qin = a.Qin[c * Np + qp];
+    o[c] = (a.wa == 0.f) ? (qin + dt * R[c]) : (a.wa * a.B[c * Np + qp] + a.wb * (qin + dt * R[c]));
   }
   o[0] = fmaxf(o[0], 1e-4f);  // positivity clamps (src/air_cfd.js:247-249)
   const float ke = 0.5f * (o[1] * o[1] + o[2] * o[2] + o[3] * o[3]) / o[0];
   if (kGm * (o[4] - ke) < 1e-5f) o[4] = 1e-5f / kGm + ke;
-  for (int c = 0; c < 5; c++) a.Out[c * Np + q] = o[c];
+  for (int c = 0; c < 5; c++) a.Out[c * Np + qp] = o[c];
 }
 
 int blocks_for(long work, int threads = 256) {
@@ -174,11 +176,12 @@ void prim_of(const double U[5], float P[5]) {  // cfdPrim5 in float64, rounded t
 int launch_march(a3d_solver* s, const StageArgs& a);  // stage_march.cu
 
 void fill_stage_args(a3d_solver* s, StageArgs& a, const float* Qin, const float* B, float* Out, float wa, float wb) {
-  a.Qin = Qin; a.B = B; a.Out = Out; a.Np = s->Np;
+  a.Qin = Qin; a.B = B; a.Out = Out; a.Np = s->Np; a.NXp = s->NXp;
   a.code = s->code; a.phi = s->geo.phi; a.ap0 = s->geo.ap0; a.ap1 = s->geo.ap1; a.ap2 = s->geo.ap2; a.ap3 = s->geo.ap3;
   a.rXd = s->grid.rXd; a.rYd = s->grid.rYd; a.rZd = s->grid.rZd;
   a.NX = s->grid.NX; a.NY = s->grid.NY; a.NZ = s->grid.NZ;
   a.wa = wa; a.wb = wb; a.cfl = (float)s->cfl; a.order2 = s->order == 2;
+  a.err = s->d_flag + 1;
   prim_of(s->F, a.Pff);
   for (int f = 0; f < 3; f++) {
     prim_of(s->fix[f], a.Pfix[f]);
@@ -187,6 +190,10 @@ void fill_stage_args(a3d_solver* s, StageArgs& a, const float* Qin, const float*
 }
 
 int launch_stage(a3d_solver* s, const StageArgs& a) {
+  if (s->kernel == KERNEL_TMA) {
+    const int qin_buf = a.Qin == s->buf[0] ? 0 : a.Qin == s->buf[1] ? 1 : 2;
+    return launch_tma(s, a, qin_buf, a.wa != 0.f);
+  }
   if (s->kernel == KERNEL_MARCH) return launch_march(s, a);
   k_stage_cell<<<(unsigned)((s->N + 255) / 256), 256, 0, s->st>>>(a);
   A3D_CUDA(cudaGetLastError());
@@ -195,19 +202,23 @@ int launch_stage(a3d_solver* s, const StageArgs& a) {
 
 int solver_finish_setup(a3d_solver* s) {
   const long N = s->N;
-  s->Np = round_up(N, 64);
+  s->NXp = (int)round_up(s->grid.NX, 16);
+  s->Np = round_up((long)s->NXp * s->grid.NY * s->grid.NZ, 64);
   A3D_CUDA(cudaMalloc(&s->state, 3 * 5 * s->Np * sizeof(float)));
   for (int b = 0; b < 3; b++) s->buf[b] = s->state + (long)b * 5 * s->Np;
   A3D_CUDA(cudaMemsetAsync(s->state, 0, 3 * 5 * s->Np * sizeof(float), s->st));
-  A3D_CUDA(cudaMalloc(&s->code, round_up(N, 256)));
-  k_codes<<<blocks_for(N), 256, 0, s->st>>>(s->grid.NX, s->grid.NY, s->grid.NZ, s->geo.t, s->geo.phi, s->geo.ap0,
-                                            s->geo.ap1, s->geo.ap2, s->geo.ap3, s->code);
+  A3D_CUDA(cudaMalloc(&s->code, round_up(s->Np, 256)));
+  A3D_CUDA(cudaMemsetAsync(s->code, T_GHOST, round_up(s->Np, 256), s->st));
+  k_codes<<<blocks_for(N), 256, 0, s->st>>>(s->grid.NX, s->grid.NY, s->grid.NZ, s->NXp, s->geo.t, s->geo.phi,
+                                            s->geo.ap0, s->geo.ap1, s->geo.ap2, s->geo.ap3, s->code);
   A3D_CUDA(cudaGetLastError());
   A3D_CUDA(cudaMalloc(&s->d_red, 4096 * 8 * sizeof(double)));
   A3D_CUDA(cudaMallocHost(&s->h_red, 64 * sizeof(double)));
   A3D_CUDA(cudaMalloc(&s->d_flag, 16));
-  A3D_CUDA(cudaMalloc(&s->prevR, N * sizeof(float)));
+  A3D_CUDA(cudaMemsetAsync(s->d_flag, 0, 16, s->st));
+  A3D_CUDA(cudaMalloc(&s->prevR, s->Np * sizeof(float)));
   A3D_TRY(build_force_list(s));
+  A3D_TRY(make_tensor_maps(s));
   const double F0[5] = {1, 0, 0, 0, 1 / (kGamma * (kGamma - 1))};  // src/air_cfd.js:162
   for (int c = 0; c < 5; c++) { s->F[c] = F0[c]; s->fix[0][c] = s->fix[1][c] = s->fix[2][c] = F0[c]; }
   A3D_CUDA(cudaStreamSynchronize(s->st));
@@ -333,8 +344,8 @@ extern "C" int a3d_solver_reset(a3d_solver* s) {
   clear_error();
   A3D_ARG(s, "null solver");
   A3D_CUDA(cudaSetDevice(s->device));
-  k_fill<<<blocks_for(s->N), 256, 0, s->st>>>(s->buf[s->iQ], s->Np, s->N, (float)s->F[0], (float)s->F[1],
-                                               (float)s->F[2], (float)s->F[3], (float)s->F[4]);
+  k_fill<<<blocks_for(s->Np), 256, 0, s->st>>>(s->buf[s->iQ], s->Np, (float)s->F[0], (float)s->F[1],
+                                                (float)s->F[2], (float)s->F[3], (float)s->F[4]);
   A3D_CUDA(cudaGetLastError());
   s->it = 0;
   s->havePrev = false;
@@ -373,10 +384,12 @@ extern "C" int a3d_solver_read(a3d_solver* s, float* r, float* ru, float* rv, fl
   A3D_CUDA(cudaSetDevice(s->device));
   float* dst[5] = {r, ru, rv, rw, E};
   const float* Q = s->buf[s->iQ];
+  const size_t row = s->grid.NX * sizeof(float), pitch = s->NXp * sizeof(float);
   for (int c = 0; c < 5; c++)
-    A3D_CUDA(cudaMemcpyAsync(dst[c], Q + c * s->Np, s->N * sizeof(float), cudaMemcpyDeviceToHost, s->st));
+    A3D_CUDA(cudaMemcpy2DAsync(dst[c], row, Q + c * s->Np, pitch, row, (size_t)s->grid.NY * s->grid.NZ,
+                               cudaMemcpyDeviceToHost, s->st));
   A3D_CUDA(cudaStreamSynchronize(s->st));
-  return A3D_OK;
+  return check_kernel_error(s);
 }
 
 extern "C" int a3d_solver_write(a3d_solver* s, const float* r, const float* ru, const float* rv, const float* rw,
@@ -386,8 +399,10 @@ extern "C" int a3d_solver_write(a3d_solver* s, const float* r, const float* ru, 
   A3D_CUDA(cudaSetDevice(s->device));
   const float* src[5] = {r, ru, rv, rw, E};
   float* Q = s->buf[s->iQ];
+  const size_t row = s->grid.NX * sizeof(float), pitch = s->NXp * sizeof(float);
   for (int c = 0; c < 5; c++)
-    A3D_CUDA(cudaMemcpyAsync(Q + c * s->Np, src[c], s->N * sizeof(float), cudaMemcpyHostToDevice, s->st));
+    A3D_CUDA(cudaMemcpy2DAsync(Q + c * s->Np, pitch, src[c], row, row, (size_t)s->grid.NY * s->grid.NZ,
+                               cudaMemcpyHostToDevice, s->st));
   A3D_CUDA(cudaStreamSynchronize(s->st));
   return A3D_OK;
 }
@@ -397,7 +412,7 @@ extern "C" int a3d_solver_write(a3d_solver* s, const float* r, const float* ru, 
 extern "C" int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t march_kz) {
   clear_error();
   A3D_ARG(s, "null solver");
-  A3D_ARG(kernel == KERNEL_CELL || kernel == KERNEL_MARCH, "kernel");
+  A3D_ARG(kernel == KERNEL_CELL || kernel == KERNEL_MARCH || kernel == KERNEL_TMA, "kernel");
   A3D_ARG(march_kz >= 1 && march_kz <= 1024, "march_kz");
   s->kernel = kernel;
   s->march_kz = march_kz;
@@ -416,5 +431,18 @@ extern "C" int a3d_solver_sync(a3d_solver* s) {
   A3D_ARG(s, "null solver");
   A3D_CUDA(cudaSetDevice(s->device));
   A3D_CUDA(cudaStreamSynchronize(s->st));
+  return check_kernel_error(s);
+}
+
+namespace a3d {
+int check_kernel_error(a3d_solver* s) {
+  int f = 0;
+  A3D_CUDA(cudaMemcpyAsync(&f, s->d_flag + 1, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+  A3D_CUDA(cudaStreamSynchronize(s->st));
+  if (f) {
+    set_error("a stage kernel gave up waiting for a TMA copy (bounded wait ran out)");
+    return A3D_ERR_TIMEOUT;
+  }
   return A3D_OK;
 }
+}  // namespace a3d

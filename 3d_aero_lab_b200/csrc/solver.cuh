@@ -1,5 +1,6 @@
 // solver.cuh - one solver case: device state, geometry codes, force list, reduction scratch.
 #pragma once
+#include <cuda.h>
 #include "geom.cuh"
 
 namespace a3d {
@@ -10,7 +11,8 @@ struct StageArgs {
   const float* __restrict__ B;
   float* __restrict__ Out;
   long Np;                       // component stride of the SoA state (5 components)
-  const uint8_t* __restrict__ code;
+  int NXp;                        // row pitch of the state and code arrays (NX rounded up to 16)
+  const uint8_t* __restrict__ code;  // per-cell codes, same padded layout as the state
   const float* __restrict__ phi;
   const float* __restrict__ ap0;
   const float* __restrict__ ap1;
@@ -25,6 +27,7 @@ struct StageArgs {
   float Pff[5];                   // primitive far-field state (rho, u, v, w, p)
   float Pfix[3][5];               // primitive fixed states of types 3, 4, 5
   float Ufix[3][5];               // conservative fixed states written to fixed cells
+  int* err;                       // set when a bounded wait inside a stage kernel ran out
 };
 
 // Device-side force-list entry arrays (cfdForceList).
@@ -35,7 +38,7 @@ struct ForceList {
   void* block = nullptr;
 };
 
-enum StageKernel { KERNEL_CELL = 0, KERNEL_MARCH = 1 };
+enum StageKernel { KERNEL_CELL = 0, KERNEL_MARCH = 1, KERNEL_TMA = 2 };
 
 }  // namespace a3d
 
@@ -44,7 +47,8 @@ struct a3d_solver {
   cudaStream_t st = nullptr;
   a3d::GridDev grid;
   a3d::GeomDev geo;
-  long N = 0, Np = 0;
+  long N = 0, Np = 0;             // cells; component stride (padded layout)
+  int NXp = 0;                    // row pitch: state[c*Np + (k*NY + j)*NXp + i]
   float* state = nullptr;         // 3 buffers x 5 components x Np floats
   float* buf[3] = {nullptr, nullptr, nullptr};
   int iQ = 0, iS1 = 1, iB = 2;
@@ -55,12 +59,14 @@ struct a3d_solver {
   double cfl = 0.7;
   int order = 2;
   long it = 0;
-  int kernel = a3d::KERNEL_MARCH;
+  int kernel = a3d::KERNEL_TMA;
+  CUtensorMap tmQ[3];             // TMA maps over the three state buffers
+  CUtensorMap tmC;                // TMA map over the code array
   int march_kz = 16;              // z planes per CTA of the march kernel
   // reductions
   double* d_red = nullptr;        // device partials + results
   double* h_red = nullptr;        // pinned host mirror of the results
-  int* d_flag = nullptr;          // non-finite flag
+  int* d_flag = nullptr;          // [0] non-finite flag, [1] stage-kernel wait timeout
   float* prevR = nullptr;         // density snapshot for the residual
   long prevIt = 0;
   bool havePrev = false;
@@ -71,4 +77,7 @@ int solver_finish_setup(a3d_solver* s);           // codes + force list + state 
 int launch_stage(a3d_solver* s, const StageArgs& a);
 void fill_stage_args(a3d_solver* s, StageArgs& a, const float* Qin, const float* B, float* Out, float wa, float wb);
 int build_force_list(a3d_solver* s);
+int make_tensor_maps(a3d_solver* s);
+int launch_tma(a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2);
+int check_kernel_error(a3d_solver* s);  // A3D_ERR_TIMEOUT if a stage kernel flagged a timeout
 }  // namespace a3d

@@ -40,7 +40,7 @@ __device__ __forceinline__ uint8_t load_cell(const StageArgs& a, int i, int j, i
   }
   const bool mirror = j < 0;
   const int jj = mirror ? -1 - j : j;
-  const long q = ((long)k * a.NY + jj) * a.NX + i;
+  const long q = ((long)k * a.NY + jj) * a.NXp + i;
   const uint8_t c = a.code[q];
   const int t = c & 7;
   if (t >= T_SINK) {
@@ -192,7 +192,8 @@ __global__ void __launch_bounds__(TX * TY, 2) k_stage_march(StageArgs a, int kz)
     __syncthreads();
     // ---- residual and RK update ----
     if (in_dom) {
-      const long q = ((long)k * a.NY + j) * a.NX + i;
+      const long q = ((long)k * a.NY + j) * a.NX + i;    // reference (geometry) index
+      const long qp = ((long)k * a.NY + j) * a.NXp + i;  // padded state index
       const int t = c0 & 7;
       float o[5];
       if (t != T_FLUID) {
@@ -201,7 +202,7 @@ __global__ void __launch_bounds__(TX * TY, 2) k_stage_march(StageArgs a, int kz)
           for (int c = 0; c < 5; c++) o[c] = a.Ufix[t - T_SINK][c];
         } else {
 #pragma unroll
-          for (int c = 0; c < 5; c++) o[c] = __ldg(a.B + c * Np + q);
+          for (int c = 0; c < 5; c++) o[c] = __ldg(a.B + c * Np + qp);
         }
       } else {
         const float rz = a.rZd[k];
@@ -232,14 +233,14 @@ __global__ void __launch_bounds__(TX * TY, 2) k_stage_march(StageArgs a, int kz)
         }
         float qin[5];
 #pragma unroll
-        for (int c = 0; c < 5; c++) qin[c] = __ldg(a.Qin + c * Np + q);
+        for (int c = 0; c < 5; c++) qin[c] = __ldg(a.Qin + c * Np + qp);
         float Pb[5], bq[5];
         if (a.wa == 0.f) {
 #pragma unroll
           for (int c = 0; c < 5; c++) { Pb[c] = W0[c]; bq[c] = 0.f; }
         } else {
 #pragma unroll
-          for (int c = 0; c < 5; c++) bq[c] = __ldg(a.B + c * Np + q);
+          for (int c = 0; c < 5; c++) bq[c] = __ldg(a.B + c * Np + qp);
           cons_to_prim(bq[0], bq[1], bq[2], bq[3], bq[4], Pb);
         }
         const float as = sqrtf(kG * Pb[4] / Pb[0]);
@@ -252,7 +253,7 @@ __global__ void __launch_bounds__(TX * TY, 2) k_stage_march(StageArgs a, int kz)
         if (kGm * (o[4] - ke) < 1e-5f) o[4] = 1e-5f / kGm + ke;
       }
 #pragma unroll
-      for (int c = 0; c < 5; c++) a.Out[c * Np + q] = o[c];
+      for (int c = 0; c < 5; c++) a.Out[c * Np + qp] = o[c];
     }
     // ---- shift the window ----
 #pragma unroll

@@ -1,0 +1,403 @@
+// stage_tma.cu - the z-marching RK-stage kernel fed by TMA (KERNEL_TMA, the default).
+//
+// Same tiling as stage_march.cu - a CTA owns 32 x 8 cell columns and walks a run of z
+// planes, evaluating every face once - but the planes arrive through a 4-deep ring of
+// shared-memory slots filled by `cp.async.bulk.tensor` (one 40 x 12 x 5-component state
+// box and one 64 x 12 code box per plane, completing on the slot's mbarrier).  While the
+// CTA computes plane k, planes k+1 .. k+3 are already resident or in flight, so no global
+// load latency sits on the critical path except the stage-2 base state, which is
+// prefetched into registers a full plane ahead of its use.
+//
+// Per plane k:
+//   wait for plane k+2; column primitives of k+2 into the register window;
+//   plane-k primitives (interior from registers, halo from the slot) to shared memory;
+//   barrier; issue the TMA of plane k+3 into the slot plane k-1 has left;
+//   x and y face fluxes from shared memory, z face k+1/2 from the register window;
+//   barrier; residual, local dt, RK update, clamps, store.
+#include <cudaTypedefs.h>
+#include "flux.cuh"
+#include "solver.cuh"
+#include "tma.cuh"
+
+namespace a3d {
+
+namespace {
+
+constexpr int TX = 32, TY = 8, HX = TX + 4, HY = TY + 4;
+constexpr int QBX = 40;  // state box width: x from i0-4 (16-byte aligned start)
+constexpr int CBX = 64;  // code box width: x from i0-16
+constexpr int NSLOT = 4;
+constexpr uint32_t kQBytes = 5 * HY * QBX * 4, kCBytes = HY * CBX;
+
+struct __align__(128) Slot {
+  float Q[5][HY][QBX];  // conservative state of one plane
+  uint8_t C[HY][CBX];   // codes of that plane
+};
+
+struct TmaSmem {
+  Slot slot[NSLOT];
+  float P[5][HY][HX];       // plane-k primitives with a 2-cell halo
+  uint8_t C[HY][HX];        // plane-k codes (ghosts marked)
+  float Fx[5][TY][TX + 1];  // a * flux of x face i-1/2
+  float Fy[5][TY + 1][TX];  // a * flux of y face j-1/2
+  float Ax[TY][TX + 1];
+  float Ay[TY + 1][TX];
+  uint64_t bar[NSLOT];
+  int abort;
+};
+
+// Primitive state and code of cell (i, j) of a resident plane k, with the ghost rules of
+// src/air_cfd.js:205-210 (far field outside x, z and +y; mirror with v negated below y = 0).
+__device__ __forceinline__ uint8_t slot_cell(const StageArgs& a, const Slot& s, int i, int j, int k, int i0, int j0,
+                                             float P[5]) {
+  if (i < 0 || i >= a.NX || k < 0 || k >= a.NZ || j >= a.NY) {
+#pragma unroll
+    for (int v = 0; v < 5; v++) P[v] = a.Pff[v];
+    return T_GHOST;
+  }
+  const bool mirror = j < 0;
+  const int y = (mirror ? -1 - j : j) - j0 + 2, xq = i - i0 + 4;
+  const uint8_t c = s.C[y][i - i0 + 16];
+  const int t = c & 7;
+  if (t >= T_SINK) {
+#pragma unroll
+    for (int v = 0; v < 5; v++) P[v] = a.Pfix[t - T_SINK][v];
+  } else {
+    cons_to_prim(s.Q[0][y][xq], s.Q[1][y][xq], s.Q[2][y][xq], s.Q[3][y][xq], s.Q[4][y][xq], P);
+  }
+  if (mirror) { P[2] = -P[2]; return T_MIRROR; }
+  return c;
+}
+
+__device__ __forceinline__ Prim sprim(const TmaSmem& S, int y, int x, int d) {
+  float P[5] = {S.P[0][y][x], S.P[1][y][x], S.P[2][y][x], S.P[3][y][x], S.P[4][y][x]};
+  return rot(P, d);
+}
+
+__device__ __forceinline__ float face_x(const StageArgs& a, const TmaSmem& S, int y, int x, int i, int j, int k,
+                                        float G[5]) {
+  const uint8_t cl = S.C[y][x - 1], cr = S.C[y][x];
+  float A = 1.f;
+  if (i - 1 >= 0 && (cl & C_IRR)) A = __ldg(a.ap0 + ((long)k * a.NY + j) * a.NX + (i - 1));
+  if (A > 0.f) {
+    float F[5];
+    face_flux(sprim(S, y, x - 2, 0), sprim(S, y, x - 1, 0), sprim(S, y, x, 0), sprim(S, y, x + 1, 0),
+              a.order2 && (cl & C_OKX), a.order2 && (cr & C_OKX), F);
+    G[0] = A * F[0]; G[1] = A * F[1]; G[2] = A * F[2]; G[3] = A * F[3]; G[4] = A * F[4];
+  } else {
+    G[0] = G[1] = G[2] = G[3] = G[4] = 0.f;
+  }
+  return A;
+}
+
+__device__ __forceinline__ float face_y(const StageArgs& a, const TmaSmem& S, int y, int x, int i, int j, int k,
+                                        float G[5]) {
+  const uint8_t cl = S.C[y - 1][x], cr = S.C[y][x];
+  float A = 1.f;
+  if (j - 1 >= 0 && (cl & C_IRR)) A = __ldg(a.ap1 + ((long)k * a.NY + (j - 1)) * a.NX + i);
+  if (A > 0.f) {
+    float F[5];
+    face_flux(sprim(S, y - 2, x, 1), sprim(S, y - 1, x, 1), sprim(S, y, x, 1), sprim(S, y + 1, x, 1),
+              a.order2 && (cl & C_OKY), a.order2 && (cr & C_OKY), F);
+    G[0] = A * F[0]; G[1] = A * F[2]; G[2] = A * F[1]; G[3] = A * F[3]; G[4] = A * F[4];
+  } else {
+    G[0] = G[1] = G[2] = G[3] = G[4] = 0.f;
+  }
+  return A;
+}
+
+__device__ __forceinline__ float face_z(const StageArgs& a, const float Pa[5], const float Pb[5], const float Pc[5],
+                                        const float Pe[5], uint8_t cb, uint8_t cc, bool in_dom_b, long qb, float G[5]) {
+  float A = 1.f;
+  if (in_dom_b && (cb & C_IRR)) A = __ldg(a.ap2 + qb);
+  if (A > 0.f) {
+    float F[5];
+    face_flux(rot(Pa, 2), rot(Pb, 2), rot(Pc, 2), rot(Pe, 2), a.order2 && (cb & C_OKZ), a.order2 && (cc & C_OKZ), F);
+    G[0] = A * F[0]; G[1] = A * F[2]; G[2] = A * F[3]; G[3] = A * F[1]; G[4] = A * F[4];
+  } else {
+    G[0] = G[1] = G[2] = G[3] = G[4] = 0.f;
+  }
+  return A;
+}
+
+// Slot of plane p for a CTA whose run starts at k0 (the ring starts with plane k0-2), and the
+// mbarrier phase parity of that use of the slot.
+__device__ __forceinline__ int slot_of(int p, int k0) { return (p - k0 + 2) & (NSLOT - 1); }
+__device__ __forceinline__ uint32_t parity_of(int p, int k0) { return ((p - k0 + 2) / NSLOT) & 1; }
+
+// Thread 0 queues plane p into its slot: one state box and one code box, or a bare arrive
+// when the plane lies outside the domain (its cells are then all far-field ghosts).
+__device__ __forceinline__ void issue_plane(TmaSmem& S, const CUtensorMap* tmQ, const CUtensorMap* tmC,
+                                            const StageArgs& a, int p, int k0, int i0, int j0) {
+  const int s = slot_of(p, k0);
+  if (p < 0 || p >= a.NZ) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&S.bar[s])) : "memory");
+    return;
+  }
+  mbar_expect_tx(&S.bar[s], kQBytes + kCBytes);
+  tma_load_4d(&S.slot[s].Q[0][0][0], tmQ, &S.bar[s], i0 - 4, j0 - 2, p, 0);
+  tma_load_3d(&S.slot[s].C[0][0], tmC, &S.bar[s], i0 - 16, j0 - 2, p);
+}
+
+// A wait ran out: flag the error for the host and wait (bounded) for the copies this CTA
+// still has in flight, so that none lands in shared memory after the CTA has left.
+__device__ void drain(TmaSmem& S, const StageArgs& a, int k0, int first_pending, int last_issued) {
+  if (threadIdx.x != 0) return;
+  atomicOr(a.err, 1);
+  for (int p = first_pending; p <= last_issued; p++) mbar_wait(&S.bar[slot_of(p, k0)], parity_of(p, k0));
+}
+
+template <bool STAGE2>
+__global__ void __launch_bounds__(TX * TY, 2)
+    k_stage_tma(const __grid_constant__ CUtensorMap tmQ, const __grid_constant__ CUtensorMap tmC, StageArgs a,
+                int kz) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  TmaSmem& S = *reinterpret_cast<TmaSmem*>(smem_raw);
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int i0 = blockIdx.x * TX, j0 = blockIdx.y * TY;
+  const int i = i0 + tx, j = j0 + ty;
+  const int k0 = blockIdx.z * kz, k1 = min(a.NZ, k0 + kz);
+  const bool in_dom = i < a.NX && j < a.NY;
+  const long NXY = (long)a.NX * a.NY, Np = a.Np;
+  const float rx = in_dom ? a.rXd[i] : 0.f, ry = in_dom ? a.rYd[j] : 0.f;
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < NSLOT; s++) mbar_init(&S.bar[s], 1);
+    S.abort = 0;
+    fence_barrier_init();
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int p = k0 - 2; p <= k0 + 1; p++) issue_plane(S, &tmQ, &tmC, a, p, k0, i0, j0);
+
+  bool ok = true;
+  float Wm[5], W0[5], W1[5], W2[5];
+  uint8_t cm, c0, c1, c2;
+  float Gz[5], Az = 1.f;
+  {
+    float Wa[5];
+    ok &= mbar_wait(&S.bar[slot_of(k0 - 2, k0)], parity_of(k0 - 2, k0));
+    slot_cell(a, S.slot[slot_of(k0 - 2, k0)], i, j, k0 - 2, i0, j0, Wa);
+    ok &= mbar_wait(&S.bar[slot_of(k0 - 1, k0)], parity_of(k0 - 1, k0));
+    cm = slot_cell(a, S.slot[slot_of(k0 - 1, k0)], i, j, k0 - 1, i0, j0, Wm);
+    ok &= mbar_wait(&S.bar[slot_of(k0, k0)], parity_of(k0, k0));
+    c0 = slot_cell(a, S.slot[slot_of(k0, k0)], i, j, k0, i0, j0, W0);
+    ok &= mbar_wait(&S.bar[slot_of(k0 + 1, k0)], parity_of(k0 + 1, k0));
+    c1 = slot_cell(a, S.slot[slot_of(k0 + 1, k0)], i, j, k0 + 1, i0, j0, W1);
+#pragma unroll
+    for (int c = 0; c < 5; c++) Gz[c] = 0.f;
+    if (in_dom) Az = face_z(a, Wa, Wm, W0, W1, cm, c0, k0 - 1 >= 0, ((long)(k0 - 1) * a.NY + j) * a.NX + i, Gz);
+  }
+  if (!ok) S.abort = 1;
+  __syncthreads();  // slots of planes k0-2 and k0-1 are free again
+  int last_issued = k0 + 1;  // meaningful in thread 0, which issues every copy
+  int first_pending = k0 - 2;
+  if (S.abort) {
+    drain(S, a, k0, first_pending, last_issued);
+    return;
+  }
+  if (threadIdx.x == 0) issue_plane(S, &tmQ, &tmC, a, k0 + 2, k0, i0, j0);
+  last_issued = k0 + 2;
+
+  for (int k = k0; k < k1; k++) {
+    const long q = ((long)k * a.NY + j) * a.NX + i;    // geometry (reference) index
+    const long qp = ((long)k * a.NY + j) * a.NXp + i;  // padded state index
+    float bq[5];
+    if (STAGE2 && in_dom) {
+#pragma unroll
+      for (int c = 0; c < 5; c++) bq[c] = __ldg(a.B + c * Np + qp);
+    }
+    // ---- plane k+2 into the column window; plane k to shared memory ----
+    const int sk = slot_of(k, k0), sk2 = slot_of(k + 2, k0);
+    ok = mbar_wait(&S.bar[sk2], parity_of(k + 2, k0));
+    c2 = slot_cell(a, S.slot[sk2], i, j, k + 2, i0, j0, W2);
+#pragma unroll
+    for (int v = 0; v < 5; v++) S.P[v][ty + 2][tx + 2] = W0[v];
+    S.C[ty + 2][tx + 2] = c0;
+    if (threadIdx.x < 160) {
+      int hx, hy;
+      const int h = threadIdx.x;
+      if (h < 32) { hy = 2 + (h >> 2); const int c = h & 3; hx = c < 2 ? c : TX + c; }
+      else { const int g = h - 32; const int r = g >> 5; hy = r < 2 ? r : TY + r; hx = 2 + (g & 31); }
+      float P[5];
+      const uint8_t c = slot_cell(a, S.slot[sk], i0 + hx - 2, j0 + hy - 2, k, i0, j0, P);
+#pragma unroll
+      for (int v = 0; v < 5; v++) S.P[v][hy][hx] = P[v];
+      S.C[hy][hx] = c;
+    }
+    if (!ok) S.abort = 1;
+    __syncthreads();
+    if (S.abort) { first_pending = k + 2; break; }
+    if (k + 3 <= k1 + 1) {
+      if (threadIdx.x == 0) {
+        fence_proxy_async_smem();
+        issue_plane(S, &tmQ, &tmC, a, k + 3, k0, i0, j0);
+      }
+      last_issued = k + 3;
+    }
+    // ---- face fluxes ----
+    if (j < a.NY && i <= a.NX) {
+      float G[5];
+      const float A = face_x(a, S, ty + 2, tx + 2, i, j, k, G);
+#pragma unroll
+      for (int v = 0; v < 5; v++) S.Fx[v][ty][tx] = G[v];
+      S.Ax[ty][tx] = A;
+    }
+    if (i < a.NX && j <= a.NY) {
+      float G[5];
+      const float A = face_y(a, S, ty + 2, tx + 2, i, j, k, G);
+#pragma unroll
+      for (int v = 0; v < 5; v++) S.Fy[v][ty][tx] = G[v];
+      S.Ay[ty][tx] = A;
+    }
+    if (ty == TY - 1) {  // +y edge faces of the tile
+      const int jj = j0 + TY;
+      if (i < a.NX && jj - 1 < a.NY) {
+        float G[5];
+        const float A = face_y(a, S, TY + 2, tx + 2, i, jj, k, G);
+#pragma unroll
+        for (int v = 0; v < 5; v++) S.Fy[v][TY][tx] = G[v];
+        S.Ay[TY][tx] = A;
+      }
+    } else if (ty == TY - 2 && tx < TY) {  // +x edge faces, one per row
+      const int row = tx, ii = i0 + TX, jr = j0 + row;
+      if (jr < a.NY && ii - 1 < a.NX) {
+        float G[5];
+        const float A = face_x(a, S, row + 2, TX + 2, ii, jr, k, G);
+#pragma unroll
+        for (int v = 0; v < 5; v++) S.Fx[v][row][TX] = G[v];
+        S.Ax[row][TX] = A;
+      }
+    }
+    float Gn[5], An = 1.f;
+    if (in_dom) An = face_z(a, Wm, W0, W1, W2, c0, c1, true, q, Gn);
+    __syncthreads();
+    // ---- residual and RK update ----
+    if (in_dom) {
+      const int t = c0 & 7;
+      float o[5];
+      const Slot& sl = S.slot[sk];
+      if (t != T_FLUID) {
+        if (t >= T_SINK) {
+#pragma unroll
+          for (int c = 0; c < 5; c++) o[c] = a.Ufix[t - T_SINK][c];
+        } else if (STAGE2) {
+#pragma unroll
+          for (int c = 0; c < 5; c++) o[c] = bq[c];
+        } else {
+#pragma unroll
+          for (int c = 0; c < 5; c++) o[c] = sl.Q[c][ty + 2][tx + 4];
+        }
+      } else {
+        const float rz = a.rZd[k];
+        const float pC = W0[4];
+        float R[5];
+#pragma unroll
+        for (int c = 0; c < 5; c++)
+          R[c] = (S.Fx[c][ty][tx] - S.Fx[c][ty][tx + 1]) * rx + (S.Fy[c][ty][tx] - S.Fy[c][ty + 1][tx]) * ry +
+                 (Gz[c] - Gn[c]) * rz;
+        R[1] += pC * (S.Ax[ty][tx + 1] - S.Ax[ty][tx]) * rx;  // wall-pressure source
+        R[2] += pC * (S.Ay[ty + 1][tx] - S.Ay[ty][tx]) * ry;
+        R[3] += pC * (An - Az) * rz;
+        if (c0 & C_BAF) {  // baffle transpiration w = u dz/dx (src/air_cfd.js:226-233)
+          const float sUp = __ldg(a.ap3 + q), sDn = k > 0 ? __ldg(a.ap3 + q - NXY) : 0.f;
+          if (sUp != 0.f || sDn != 0.f) {
+            const float r = W0[0], u = W0[1], v = W0[2], w = W0[3];
+            const float Hh = (pC / kGm + 0.5f * r * (u * u + v * v + w * w) + pC) / r;
+            const float m = (sDn != 0.f ? (1.f - Az) * r * u * sDn : 0.f) - (sUp != 0.f ? (1.f - An) * r * u * sUp : 0.f);
+            const float mh = m * rz;
+            R[0] += mh; R[1] += mh * u; R[2] += mh * v; R[3] += mh * w; R[4] += mh * Hh;
+          }
+        }
+        const float ph = (c0 & C_IRR) ? __ldg(a.phi + q) : 1.f;
+        if (ph != 1.f) {
+          const float iph = 1.f / ph;
+#pragma unroll
+          for (int c = 0; c < 5; c++) R[c] *= iph;
+        }
+        float Pb[5];
+        if (STAGE2) cons_to_prim(bq[0], bq[1], bq[2], bq[3], bq[4], Pb);
+        else {
+#pragma unroll
+          for (int c = 0; c < 5; c++) Pb[c] = W0[c];
+        }
+        const float as = sqrtf(kG * Pb[4] / Pb[0]);
+        const float dt = a.cfl * fmaxf(ph, 0.25f) /
+                         ((fabsf(Pb[1]) + as) * rx + (fabsf(Pb[2]) + as) * ry + (fabsf(Pb[3]) + as) * rz);
+#pragma unroll
+        for (int c = 0; c < 5; c++) {
+          const float qin = sl.Q[c][ty + 2][tx + 4];
+          o[c] = STAGE2 ? (a.wa * bq[c] + a.wb * (qin + dt * R[c])) : (qin + dt * R[c]);
+        }
+        o[0] = fmaxf(o[0], 1e-4f);  // positivity clamps (src/air_cfd.js:247-249)
+        const float ke = 0.5f * (o[1] * o[1] + o[2] * o[2] + o[3] * o[3]) / o[0];
+        if (kGm * (o[4] - ke) < 1e-5f) o[4] = 1e-5f / kGm + ke;
+      }
+#pragma unroll
+      for (int c = 0; c < 5; c++) a.Out[c * Np + qp] = o[c];
+    }
+#pragma unroll
+    for (int c = 0; c < 5; c++) { Gz[c] = Gn[c]; Wm[c] = W0[c]; W0[c] = W1[c]; W1[c] = W2[c]; }
+    Az = An;
+    cm = c0; c0 = c1; c1 = c2;
+    (void)cm;
+  }
+  if (S.abort) drain(S, a, k0, first_pending, last_issued);
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  if (!fn) {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  }
+  return fn;
+}
+
+}  // namespace
+
+size_t tma_smem_bytes() { return sizeof(TmaSmem) + 128; }
+
+// Tensor maps over the padded state buffers (x, y, z, component) and the code array (x, y, z).
+int make_tensor_maps(a3d_solver* s) {
+  auto enc = encode_fn();
+  if (!enc) { set_error("cuTensorMapEncodeTiled is not available from the driver"); return A3D_ERR_CUDA; }
+  const cuuint64_t NX = s->grid.NX, NY = s->grid.NY, NZ = s->grid.NZ, NXp = s->NXp;
+  for (int b = 0; b < 3; b++) {
+    const cuuint64_t dims[4] = {NX, NY, NZ, 5};
+    const cuuint64_t strides[3] = {NXp * 4, NXp * NY * 4, (cuuint64_t)s->Np * 4};
+    const cuuint32_t box[4] = {QBX, HY, 1, 5}, es[4] = {1, 1, 1, 1};
+    CUresult r = enc(&s->tmQ[b], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, s->buf[b], dims, strides, box, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) { set_error("cuTensorMapEncodeTiled(state) failed: %d", (int)r); return A3D_ERR_CUDA; }
+  }
+  const cuuint64_t cd[3] = {NX, NY, NZ}, cs[2] = {NXp, NXp * NY};
+  const cuuint32_t cb[3] = {CBX, HY, 1}, ce[3] = {1, 1, 1};
+  CUresult r = enc(&s->tmC, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, s->code, cd, cs, cb, ce, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) { set_error("cuTensorMapEncodeTiled(codes) failed: %d", (int)r); return A3D_ERR_CUDA; }
+  static bool attr = false;
+  if (!attr) {
+    A3D_CUDA(cudaFuncSetAttribute(k_stage_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem_bytes()));
+    A3D_CUDA(cudaFuncSetAttribute(k_stage_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem_bytes()));
+    attr = true;
+  }
+  return A3D_OK;
+}
+
+int launch_tma(a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2) {
+  const int kz = s->march_kz;
+  dim3 grid((a.NX + TX - 1) / TX, (a.NY + TY - 1) / TY, (a.NZ + kz - 1) / kz);
+  if (stage2)
+    k_stage_tma<true><<<grid, TX * TY, tma_smem_bytes(), s->st>>>(s->tmQ[qin_buf], s->tmC, a, kz);
+  else
+    k_stage_tma<false><<<grid, TX * TY, tma_smem_bytes(), s->st>>>(s->tmQ[qin_buf], s->tmC, a, kz);
+  A3D_CUDA(cudaGetLastError());
+  return A3D_OK;
+}
+
+}  // namespace a3d
