@@ -56,6 +56,7 @@ PROTOS = {
     "a3d_solver_set_kernel": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "a3d_solver_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
     "a3d_solver_sync": (C.c_int, [_vp]),
+    "a3d_forces_noalloc": (C.c_int, [_vp] * 5 + [C.c_int64] + [_vp] * 5 + [C.c_double] * 6 + [_vp, _dp]),
 }
 
 _lib = None

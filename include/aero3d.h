@@ -170,6 +170,25 @@ int a3d_solver_stream(a3d_solver* s, void** stream);
 /* Blocks until all work queued on the solver's stream has finished. */
 int a3d_solver_sync(a3d_solver* s);
 
+/* ---- force integral without device allocation ------------------------------------- */
+/* No counterpart in the reference.  The same C_L, C_D, C_m as a3d_solver_forces, for callers
+ * that hold the state and the force list in device memory of their own and cannot call
+ * cudaMalloc (a host application that gives the addon a fixed device pool, or code that must
+ * not change the device's allocation state).  Inputs: five device arrays of the conservative
+ * state indexed by the reference cell index q, and the device force list (q, cx, cz, x, z) of
+ * n cells, as a3d_solver_force_list returns it.  Scratch is a static device array inside the
+ * library (about 96 KiB per GPU that loads it, held until exit), so n is limited to 1,048,576
+ * list cells; longer lists are rejected with A3D_ERR_ARG.  The call allocates and frees
+ * nothing.  The first call on a device looks up the scratch address on that device (make it
+ * before any stream capture).  All calls share the scratch: calls that overlap on the GPU
+ * (different streams, or several host threads at once) race.  Work is queued on `stream`
+ * (NULL: the default stream) and the call waits for it; out = {CL, CD, Cm}.            */
+int a3d_forces_noalloc(const float* r, const float* ru, const float* rv, const float* rw,
+                       const float* E, int64_t n, const int64_t* q, const double* cx,
+                       const double* cz, const double* x, const double* z,
+                       double alpha_deg, double M, double S, double xcg, double zcg,
+                       double cref, void* stream, double out[3]);
+
 #ifdef __cplusplus
 }
 #endif
