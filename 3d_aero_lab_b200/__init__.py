@@ -11,7 +11,7 @@ from .aircraft import build_aircraft, shape_of, trefftz_x  # noqa: F401
 
 def __getattr__(name):
     # the solver surface loads libaero3d.so on first use and raises if it cannot
-    if name in ("cfd", "CfdGPU", "Case", "cfd_grid", "cfd_geom", "freestream", "AeroError"):
+    if name in ("cfd", "CfdGPU", "Case", "Batch", "cfd_grid", "cfd_geom", "freestream", "AeroError"):
         import importlib
         cfd = importlib.import_module(__name__ + ".cfd")
         _lib = importlib.import_module(__name__ + "._lib")

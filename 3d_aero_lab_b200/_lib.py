@@ -9,7 +9,7 @@ import os
 
 import numpy as np
 
-from .abi import STATUS_NAMES, a3d_shape
+from .abi import STATUS_NAMES, a3d_request, a3d_result, a3d_server_config, a3d_shape
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libaero3d.so")
@@ -56,6 +56,20 @@ PROTOS = {
     "a3d_solver_set_kernel": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "a3d_solver_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
     "a3d_solver_sync": (C.c_int, [_vp]),
+    "a3d_batch_create": (C.c_int, [C.POINTER(_vp), C.c_int32, C.POINTER(_vp)]),
+    "a3d_batch_destroy": (C.c_int, [_vp]),
+    "a3d_batch_step": (C.c_int, [_vp, C.c_int32]),
+    "a3d_batch_sync": (C.c_int, [_vp]),
+    "a3d_batch_set_schedule": (C.c_int, [_vp, C.c_int32, C.c_int32]),
+    "a3d_batch_get_schedule": (C.c_int, [_vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
+    "a3d_batch_tune": (C.c_int, [_vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                 C.POINTER(C.c_float)]),
+    "a3d_server_create": (C.c_int, [C.POINTER(a3d_server_config), C.POINTER(_vp)]),
+    "a3d_server_submit": (C.c_int, [_vp, C.POINTER(a3d_request), C.POINTER(C.c_int64)]),
+    "a3d_server_poll": (C.c_int, [_vp, C.c_int64, C.POINTER(a3d_result), C.POINTER(C.c_int32)]),
+    "a3d_server_wait": (C.c_int, [_vp, C.c_int64, C.c_double, C.POINTER(a3d_result)]),
+    "a3d_server_stats": (C.c_int, [_vp, _i64]),
+    "a3d_server_destroy": (C.c_int, [_vp]),
     "a3d_forces_noalloc": (C.c_int, [_vp] * 5 + [C.c_int64] + [_vp] * 5 + [C.c_double] * 6 + [_vp, _dp]),
 }
 

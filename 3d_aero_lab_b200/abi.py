@@ -35,3 +35,23 @@ class a3d_shape(C.Structure):
                 ("ref_b", C.c_double), ("view_Rmax", C.c_double), ("lip_x", C.c_double), ("lip_r", C.c_double),
                 ("n_engines", C.c_int32), ("n_exits", C.c_int32),
                 ("engines", a3d_engine * A3D_MAX_ENGINES), ("exits", a3d_exit * A3D_MAX_EXITS)]
+
+
+class a3d_server_config(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_double), ("residual_drop", C.c_double), ("max_active", C.c_int32),
+                ("chunk_iters", C.c_int32), ("max_iters", C.c_int32), ("device", C.c_int32),
+                ("warm_start", C.c_int32), ("kz", C.c_int32)]
+
+
+class a3d_request(C.Structure):
+    _fields_ = [("shape", a3d_shape), ("cells", C.c_double), ("M", C.c_double), ("alpha_deg", C.c_double),
+                ("delta_deg", C.c_double), ("F", C.c_double * 5), ("fix", C.c_double * 15),
+                ("ref_S", C.c_double), ("ref_xcg", C.c_double), ("ref_zcg", C.c_double), ("ref_c", C.c_double),
+                ("xT", C.c_double), ("geometry_key", C.c_uint64)]
+
+
+class a3d_result(C.Structure):
+    _fields_ = [("status", C.c_int32), ("warm", C.c_int32), ("iterations", C.c_int64),
+                ("CL", C.c_double), ("CD", C.c_double), ("Cm", C.c_double), ("CDi", C.c_double),
+                ("residual", C.c_double), ("res0", C.c_double),
+                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double)]

@@ -258,3 +258,43 @@ class Case:
 
     def trefftz(self):
         return self.solver.trefftz(self.xT, self.alpha, self.M, self.ac.ref["S"])
+
+
+class Batch:
+    """Many solver cases advanced together: one persistent launch per RK stage (a3d_batch_*)."""
+
+    def __init__(self, solvers):
+        self.solvers = list(solvers)
+        arr = (C.c_void_p * len(self.solvers))(*[s._h.value for s in self.solvers])
+        self._h = C.c_void_p()
+        _lib.check(_lib.lib().a3d_batch_create(arr, len(self.solvers), C.byref(self._h)))
+
+    def step(self, n):
+        _lib.check(_lib.lib().a3d_batch_step(self._h, int(n)))
+
+    def sync(self):
+        _lib.check(_lib.lib().a3d_batch_sync(self._h))
+
+    def tune(self, trial_iters=20):
+        kz, ct, ms = C.c_int32(), C.c_int32(), C.c_float()
+        _lib.check(_lib.lib().a3d_batch_tune(self._h, int(trial_iters), C.byref(kz), C.byref(ct), C.byref(ms)))
+        return {"kz": kz.value, "ctas_per_sm": ct.value, "ms_per_iteration": ms.value}
+
+    def set_schedule(self, kz, ctas_per_sm):
+        _lib.check(_lib.lib().a3d_batch_set_schedule(self._h, int(kz), int(ctas_per_sm)))
+
+    def schedule(self):
+        kz, ct, tiles = C.c_int32(), C.c_int32(), C.c_int64()
+        _lib.check(_lib.lib().a3d_batch_get_schedule(self._h, C.byref(kz), C.byref(ct), C.byref(tiles)))
+        return {"kz": kz.value, "ctas_per_sm": ct.value, "tiles": tiles.value}
+
+    def dispose(self):
+        if self._h:
+            _lib.lib().a3d_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.dispose()
+        except Exception:
+            pass

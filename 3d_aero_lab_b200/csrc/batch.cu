@@ -1,0 +1,315 @@
+// batch.cu - many cases of uneven size in one persistent launch per RK stage.
+//
+// A batch groups solver objects (each with its own grid, geometry and state) on one device.
+// A device table holds, per case, its TMA maps, stage constants, state buffers and tile
+// counts; tiles of all cases are numbered consecutively (largest cases first).  The stage
+// kernel is persistent: a grid of (SM count x CTAs per SM) CTAs pulls tile numbers from a
+// global counter and runs the same fused tile as the single-case kernel (stage_fused.cuh).
+// The last CTA to find the queue empty resets the counter, so the four launches of two
+// SSP-RK2 iterations are captured once in a CUDA graph and replayed; buffer roles alternate
+// with the iteration's parity (Q and B swap every iteration, as in src/air_cfd.js:256).
+// The autotuner times candidate z-run lengths per tile and CTA counts on the real batch
+// (state saved and restored around the trials) and keeps the fastest.
+#include <algorithm>
+#include <numeric>
+#include <vector>
+#include "stage_fused.cuh"
+
+namespace a3d {
+
+namespace {
+
+using namespace fused;
+
+struct __align__(128) BatchCase {
+  CUtensorMap tmQ[3];  // maps over the case's three state buffers
+  CUtensorMap tmC;     // map over its codes
+  StageArgs a;         // stage constants (pointers, dims, far-field/fixed states, cfl, order)
+  float* buf[3];
+  int iQ, iS1, iB;     // buffer roles at the start of the batch step
+  int nbx, nby, nbz, kz;
+  long long tile_begin;
+};
+
+template <bool STAGE2>
+__global__ void __launch_bounds__(TX * TY, 2)
+    k_batch_stage(const BatchCase* __restrict__ cases, int ncases, long long total, int parity,
+                  unsigned long long* counter) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  FusedSmem& S = *reinterpret_cast<FusedSmem*>(smem_raw);
+  __shared__ long long s_w;
+  for (;;) {
+    if (threadIdx.x == 0) s_w = (long long)atomicAdd(counter, 1ULL);
+    __syncthreads();
+    const long long w = s_w;
+    __syncthreads();
+    if (w >= total) {
+      // every CTA takes exactly one ticket past the end; the last one resets the queue
+      if (threadIdx.x == 0 && w == total + (long long)gridDim.x - 1) *counter = 0ULL;
+      return;
+    }
+    int lo = 0, hi = ncases - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (cases[mid].tile_begin <= w) lo = mid; else hi = mid - 1;
+    }
+    const BatchCase& C = cases[lo];
+    const long long t = w - C.tile_begin;
+    const int bx = (int)(t % C.nbx), by = (int)((t / C.nbx) % C.nby), bz = (int)(t / ((long long)C.nbx * C.nby));
+    const int iq = parity ? C.iB : C.iQ, ib = parity ? C.iQ : C.iB;
+    // stage 1: S1 = Q + dt R(Q); stage 2: B = Q/2 + (S1 + dt R(S1))/2
+    const int qin = STAGE2 ? C.iS1 : iq;
+    float* out = STAGE2 ? C.buf[ib] : C.buf[C.iS1];
+    if (!stage_tile<STAGE2>(S, &C.tmQ[qin], &C.tmC, C.a, C.buf[iq], out, bx, by, bz, C.kz)) return;
+  }
+}
+
+}  // namespace
+
+}  // namespace a3d
+
+struct a3d_batch {
+  int device = 0;
+  int n_sm = 148;
+  cudaStream_t st = nullptr;
+  std::vector<a3d_solver*> solvers;
+  std::vector<cudaEvent_t> ev_in;  // one per solver: its stream's work before the batch
+  cudaEvent_t ev_out = nullptr;
+  a3d::BatchCase* d_cases = nullptr;
+  std::vector<a3d::BatchCase> h_cases;
+  std::vector<int> order;          // solver index of each table row (largest first)
+  unsigned long long* d_counters = nullptr;
+  long long total = 0;
+  int kz = 32;
+  int ctas_per_sm = 2;
+  cudaGraphExec_t graph = nullptr;
+  bool table_dirty = true;
+};
+
+namespace a3d {
+
+namespace {
+
+void free_graph(a3d_batch* b) {
+  if (b->graph) cudaGraphExecDestroy(b->graph);
+  b->graph = nullptr;
+}
+
+int build_table(a3d_batch* b) {
+  const int n = (int)b->solvers.size();
+  b->h_cases.assign(n, BatchCase{});
+  long long tile = 0;
+  for (int r = 0; r < n; r++) {
+    a3d_solver* s = b->solvers[b->order[r]];
+    BatchCase& C = b->h_cases[r];
+    C.tmQ[0] = s->tmQ[0]; C.tmQ[1] = s->tmQ[1]; C.tmQ[2] = s->tmQ[2];
+    C.tmC = s->tmC;
+    fill_stage_args(s, C.a, nullptr, nullptr, nullptr, 0.5f, 0.5f);
+    for (int k = 0; k < 3; k++) C.buf[k] = s->buf[k];
+    C.iQ = s->iQ; C.iS1 = s->iS1; C.iB = s->iB;
+    C.kz = std::max(1, std::min(b->kz, s->grid.NZ));
+    C.nbx = (s->grid.NX + TX - 1) / TX;
+    C.nby = (s->grid.NY + TY - 1) / TY;
+    C.nbz = (s->grid.NZ + C.kz - 1) / C.kz;
+    C.tile_begin = tile;
+    tile += (long long)C.nbx * C.nby * C.nbz;
+  }
+  b->total = tile;
+  A3D_CUDA(cudaMemcpyAsync(b->d_cases, b->h_cases.data(), n * sizeof(BatchCase), cudaMemcpyHostToDevice, b->st));
+  b->table_dirty = false;
+  return A3D_OK;
+}
+
+int launch_pair(a3d_batch* b, int parity, cudaStream_t st) {
+  const int grid = b->n_sm * b->ctas_per_sm, n = (int)b->solvers.size();
+  const size_t smem = fused_smem_bytes();
+  k_batch_stage<false><<<grid, TX * TY, smem, st>>>(b->d_cases, n, b->total, parity, b->d_counters + 2 * parity);
+  k_batch_stage<true><<<grid, TX * TY, smem, st>>>(b->d_cases, n, b->total, parity, b->d_counters + 2 * parity + 1);
+  A3D_CUDA(cudaGetLastError());
+  return A3D_OK;
+}
+
+// Graph of two iterations (parities 0 and 1): four persistent launches.
+int build_graph(a3d_batch* b) {
+  free_graph(b);
+  cudaGraph_t g = nullptr;
+  A3D_CUDA(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+  int rc = launch_pair(b, 0, b->st);
+  if (rc == A3D_OK) rc = launch_pair(b, 1, b->st);
+  cudaError_t e = cudaStreamEndCapture(b->st, &g);
+  if (rc != A3D_OK) { if (g) cudaGraphDestroy(g); return rc; }
+  if (e != cudaSuccess) { set_error("graph capture: %s", cudaGetErrorString(e)); return A3D_ERR_CUDA; }
+  e = cudaGraphInstantiate(&b->graph, g, 0);
+  cudaGraphDestroy(g);
+  if (e != cudaSuccess) { set_error("graph instantiate: %s", cudaGetErrorString(e)); return A3D_ERR_CUDA; }
+  return A3D_OK;
+}
+
+// Runs n iterations of every case; updates each solver's roles and iteration count.
+int run(a3d_batch* b, int n) {
+  for (size_t k = 0; k < b->solvers.size(); k++) {  // order after each solver's own work
+    A3D_CUDA(cudaEventRecord(b->ev_in[k], b->solvers[k]->st));
+    A3D_CUDA(cudaStreamWaitEvent(b->st, b->ev_in[k], 0));
+  }
+  if (b->table_dirty) A3D_TRY(build_table(b));
+  if (!b->graph) A3D_TRY(build_graph(b));
+  for (int p = 0; p + 1 < n; p += 2) A3D_CUDA(cudaGraphLaunch(b->graph, b->st));
+  if (n & 1) A3D_TRY(launch_pair(b, 0, b->st));
+  A3D_CUDA(cudaEventRecord(b->ev_out, b->st));
+  for (a3d_solver* s : b->solvers) {
+    A3D_CUDA(cudaStreamWaitEvent(s->st, b->ev_out, 0));
+    if (n & 1) std::swap(s->iQ, s->iB);
+    s->it += n;
+  }
+  if (n & 1) b->table_dirty = true;
+  return A3D_OK;
+}
+
+}  // namespace
+
+}  // namespace a3d
+
+using namespace a3d;
+
+extern "C" int a3d_batch_create(a3d_solver* const* solvers, int32_t n, a3d_batch** out) {
+  clear_error();
+  A3D_ARG(solvers && out && n >= 1, "solvers");
+  const int dev = solvers[0]->device;
+  for (int k = 0; k < n; k++) {
+    A3D_ARG(solvers[k], "null solver");
+    A3D_ARG(solvers[k]->device == dev, "all solvers of a batch must live on one device");
+    A3D_ARG(solvers[k]->kernel == KERNEL_FUSED || solvers[k]->kernel == KERNEL_TMA, "batch needs TMA-capable solvers");
+  }
+  A3D_CUDA(cudaSetDevice(dev));
+  a3d_batch* b = new a3d_batch();
+  b->device = dev;
+  cudaDeviceGetAttribute(&b->n_sm, cudaDevAttrMultiProcessorCount, dev);
+  b->solvers.assign(solvers, solvers + n);
+  b->order.resize(n);
+  std::iota(b->order.begin(), b->order.end(), 0);
+  std::stable_sort(b->order.begin(), b->order.end(), [&](int x, int y) { return b->solvers[x]->N > b->solvers[y]->N; });
+  int rc = A3D_OK;
+  cudaError_t e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->ev_out, cudaEventDisableTiming);
+  b->ev_in.assign(n, nullptr);
+  for (int k = 0; k < n && e == cudaSuccess; k++) e = cudaEventCreateWithFlags(&b->ev_in[k], cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_cases, (size_t)n * sizeof(BatchCase));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_counters, 8 * sizeof(unsigned long long));
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->d_counters, 0, 8 * sizeof(unsigned long long), b->st);
+  if (e != cudaSuccess) { set_error("batch setup: %s", cudaGetErrorString(e)); rc = e == cudaErrorMemoryAllocation ? A3D_ERR_NOMEM : A3D_ERR_CUDA; }
+  if (rc == A3D_OK) {
+    int r = cudaFuncSetAttribute(k_batch_stage<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes());
+    if (r == cudaSuccess) r = cudaFuncSetAttribute(k_batch_stage<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes());
+    if (r != cudaSuccess) { set_error("batch kernel attributes: %s", cudaGetErrorString((cudaError_t)r)); rc = A3D_ERR_CUDA; }
+  }
+  if (rc != A3D_OK) { a3d_batch_destroy(b); return rc; }
+  *out = b;
+  return A3D_OK;
+}
+
+extern "C" int a3d_batch_destroy(a3d_batch* b) {
+  if (!b) return A3D_OK;
+  cudaSetDevice(b->device);
+  if (b->st) cudaStreamSynchronize(b->st);
+  free_graph(b);
+  cudaFree(b->d_cases);
+  cudaFree(b->d_counters);
+  for (cudaEvent_t e : b->ev_in) if (e) cudaEventDestroy(e);
+  if (b->ev_out) cudaEventDestroy(b->ev_out);
+  if (b->st) cudaStreamDestroy(b->st);
+  delete b;
+  return A3D_OK;
+}
+
+extern "C" int a3d_batch_set_schedule(a3d_batch* b, int32_t kz, int32_t ctas_per_sm) {
+  clear_error();
+  A3D_ARG(b, "null batch");
+  A3D_ARG(kz >= 1 && kz <= 1024 && ctas_per_sm >= 1 && ctas_per_sm <= 2, "schedule");
+  b->kz = kz;
+  b->ctas_per_sm = ctas_per_sm;
+  b->table_dirty = true;
+  free_graph(b);
+  return A3D_OK;
+}
+
+extern "C" int a3d_batch_get_schedule(a3d_batch* b, int32_t* kz, int32_t* ctas_per_sm, int64_t* tiles) {
+  clear_error();
+  A3D_ARG(b, "null batch");
+  if (kz) *kz = b->kz;
+  if (ctas_per_sm) *ctas_per_sm = b->ctas_per_sm;
+  if (tiles) *tiles = b->total;
+  return A3D_OK;
+}
+
+extern "C" int a3d_batch_step(a3d_batch* b, int32_t n) {
+  clear_error();
+  A3D_ARG(b && n >= 0, "batch step");
+  A3D_CUDA(cudaSetDevice(b->device));
+  return run(b, n);
+}
+
+extern "C" int a3d_batch_sync(a3d_batch* b) {
+  clear_error();
+  A3D_ARG(b, "null batch");
+  A3D_CUDA(cudaSetDevice(b->device));
+  A3D_CUDA(cudaStreamSynchronize(b->st));
+  for (a3d_solver* s : b->solvers) A3D_TRY(check_kernel_error(s));
+  return A3D_OK;
+}
+
+extern "C" int a3d_batch_tune(a3d_batch* b, int32_t trial_iters, int32_t* best_kz, int32_t* best_ctas,
+                              float* best_ms) {
+  clear_error();
+  A3D_ARG(b && trial_iters >= 2, "tune");
+  A3D_CUDA(cudaSetDevice(b->device));
+  const int n = (int)b->solvers.size();
+  const int it = trial_iters & ~1;  // even: the buffer roles come back to where they were
+  // save every case's current state and iteration count
+  std::vector<float*> saved(n, nullptr);
+  std::vector<long> saved_it(n);
+  int rc = A3D_OK;
+  for (int k = 0; k < n && rc == A3D_OK; k++) {
+    a3d_solver* s = b->solvers[k];
+    A3D_CUDA(cudaStreamSynchronize(s->st));
+    if (cudaMalloc(&saved[k], 5 * s->Np * sizeof(float)) != cudaSuccess) { set_error("tune: no memory for the state copy"); rc = A3D_ERR_NOMEM; break; }
+    A3D_CUDA(cudaMemcpyAsync(saved[k], s->buf[s->iQ], 5 * s->Np * sizeof(float), cudaMemcpyDeviceToDevice, s->st));
+    saved_it[k] = s->it;
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int bkz = b->kz, bct = b->ctas_per_sm;
+  const int kzs[] = {8, 16, 32, 64};
+  for (int ct = 1; ct <= 2 && rc == A3D_OK; ct++)
+    for (int kz : kzs) {
+      if (rc != A3D_OK) break;
+      a3d_batch_set_schedule(b, kz, ct);
+      rc = run(b, 2);  // warm: builds the table and the graph
+      if (rc != A3D_OK) break;
+      cudaEventRecord(e0, b->st);
+      rc = run(b, it);
+      cudaEventRecord(e1, b->st);
+      cudaEventSynchronize(e1);
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (ms < best) { best = ms; bkz = kz; bct = ct; }
+    }
+  if (rc == A3D_OK) rc = a3d_batch_set_schedule(b, bkz, bct);
+  for (int k = 0; k < n; k++) {  // restore
+    a3d_solver* s = b->solvers[k];
+    cudaStreamSynchronize(b->st);
+    if (saved[k]) {
+      cudaMemcpy(s->buf[s->iQ], saved[k], 5 * s->Np * sizeof(float), cudaMemcpyDeviceToDevice);
+      cudaFree(saved[k]);
+    }
+    s->it = saved_it[k];
+  }
+  b->table_dirty = true;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (best_kz) *best_kz = bkz;
+  if (best_ctas) *best_ctas = bct;
+  if (best_ms) *best_ms = best / (float)it;
+  return rc;
+}

@@ -190,9 +190,9 @@ void fill_stage_args(a3d_solver* s, StageArgs& a, const float* Qin, const float*
 }
 
 int launch_stage(a3d_solver* s, const StageArgs& a) {
-  if (s->kernel == KERNEL_TMA) {
+  if (s->kernel == KERNEL_TMA || s->kernel == KERNEL_FUSED) {
     const int qin_buf = a.Qin == s->buf[0] ? 0 : a.Qin == s->buf[1] ? 1 : 2;
-    return launch_tma(s, a, qin_buf, a.wa != 0.f);
+    return s->kernel == KERNEL_FUSED ? launch_fused(s, a, qin_buf, a.wa != 0.f) : launch_tma(s, a, qin_buf, a.wa != 0.f);
   }
   if (s->kernel == KERNEL_MARCH) return launch_march(s, a);
   k_stage_cell<<<(unsigned)((s->N + 255) / 256), 256, 0, s->st>>>(a);
@@ -412,7 +412,7 @@ extern "C" int a3d_solver_write(a3d_solver* s, const float* r, const float* ru, 
 extern "C" int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t march_kz) {
   clear_error();
   A3D_ARG(s, "null solver");
-  A3D_ARG(kernel == KERNEL_CELL || kernel == KERNEL_MARCH || kernel == KERNEL_TMA, "kernel");
+  A3D_ARG(kernel >= KERNEL_CELL && kernel <= KERNEL_FUSED, "kernel");
   A3D_ARG(march_kz >= 1 && march_kz <= 1024, "march_kz");
   s->kernel = kernel;
   s->march_kz = march_kz;

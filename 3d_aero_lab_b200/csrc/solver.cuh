@@ -38,7 +38,7 @@ struct ForceList {
   void* block = nullptr;
 };
 
-enum StageKernel { KERNEL_CELL = 0, KERNEL_MARCH = 1, KERNEL_TMA = 2 };
+enum StageKernel { KERNEL_CELL = 0, KERNEL_MARCH = 1, KERNEL_TMA = 2, KERNEL_FUSED = 3 };
 
 }  // namespace a3d
 
@@ -59,10 +59,10 @@ struct a3d_solver {
   double cfl = 0.7;
   int order = 2;
   long it = 0;
-  int kernel = a3d::KERNEL_TMA;
+  int kernel = a3d::KERNEL_FUSED;
   CUtensorMap tmQ[3];             // TMA maps over the three state buffers
   CUtensorMap tmC;                // TMA map over the code array
-  int march_kz = 16;              // z planes per CTA of the march kernel
+  int march_kz = 32;              // z planes per CTA of the marching kernels
   // reductions
   double* d_red = nullptr;        // device partials + results
   double* h_red = nullptr;        // pinned host mirror of the results
@@ -79,5 +79,8 @@ void fill_stage_args(a3d_solver* s, StageArgs& a, const float* Qin, const float*
 int build_force_list(a3d_solver* s);
 int make_tensor_maps(a3d_solver* s);
 int launch_tma(a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2);
+int launch_fused(a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2);
+size_t fused_smem_bytes();
+int fused_set_attributes();
 int check_kernel_error(a3d_solver* s);  // A3D_ERR_TIMEOUT if a stage kernel flagged a timeout
 }  // namespace a3d

@@ -18,21 +18,13 @@
 #include "flux.cuh"
 #include "solver.cuh"
 #include "tma.cuh"
+#include "tma_ring.cuh"
 
 namespace a3d {
 
 namespace {
 
-constexpr int TX = 32, TY = 8, HX = TX + 4, HY = TY + 4;
-constexpr int QBX = 40;  // state box width: x from i0-4 (16-byte aligned start)
-constexpr int CBX = 64;  // code box width: x from i0-16
-constexpr int NSLOT = 4;
-constexpr uint32_t kQBytes = 5 * HY * QBX * 4, kCBytes = HY * CBX;
-
-struct __align__(128) Slot {
-  float Q[5][HY][QBX];  // conservative state of one plane
-  uint8_t C[HY][CBX];   // codes of that plane
-};
+using namespace ring;
 
 struct TmaSmem {
   Slot slot[NSLOT];
@@ -45,29 +37,6 @@ struct TmaSmem {
   uint64_t bar[NSLOT];
   int abort;
 };
-
-// Primitive state and code of cell (i, j) of a resident plane k, with the ghost rules of
-// src/air_cfd.js:205-210 (far field outside x, z and +y; mirror with v negated below y = 0).
-__device__ __forceinline__ uint8_t slot_cell(const StageArgs& a, const Slot& s, int i, int j, int k, int i0, int j0,
-                                             float P[5]) {
-  if (i < 0 || i >= a.NX || k < 0 || k >= a.NZ || j >= a.NY) {
-#pragma unroll
-    for (int v = 0; v < 5; v++) P[v] = a.Pff[v];
-    return T_GHOST;
-  }
-  const bool mirror = j < 0;
-  const int y = (mirror ? -1 - j : j) - j0 + 2, xq = i - i0 + 4;
-  const uint8_t c = s.C[y][i - i0 + 16];
-  const int t = c & 7;
-  if (t >= T_SINK) {
-#pragma unroll
-    for (int v = 0; v < 5; v++) P[v] = a.Pfix[t - T_SINK][v];
-  } else {
-    cons_to_prim(s.Q[0][y][xq], s.Q[1][y][xq], s.Q[2][y][xq], s.Q[3][y][xq], s.Q[4][y][xq], P);
-  }
-  if (mirror) { P[2] = -P[2]; return T_MIRROR; }
-  return c;
-}
 
 __device__ __forceinline__ Prim sprim(const TmaSmem& S, int y, int x, int d) {
   float P[5] = {S.P[0][y][x], S.P[1][y][x], S.P[2][y][x], S.P[3][y][x], S.P[4][y][x]};
@@ -120,35 +89,9 @@ __device__ __forceinline__ float face_z(const StageArgs& a, const float Pa[5], c
   return A;
 }
 
-// Slot of plane p for a CTA whose run starts at k0 (the ring starts with plane k0-2), and the
-// mbarrier phase parity of that use of the slot.
-__device__ __forceinline__ int slot_of(int p, int k0) { return (p - k0 + 2) & (NSLOT - 1); }
-__device__ __forceinline__ uint32_t parity_of(int p, int k0) { return ((p - k0 + 2) / NSLOT) & 1; }
-
-// Thread 0 queues plane p into its slot: one state box and one code box, or a bare arrive
-// when the plane lies outside the domain (its cells are then all far-field ghosts).
-__device__ __forceinline__ void issue_plane(TmaSmem& S, const CUtensorMap* tmQ, const CUtensorMap* tmC,
-                                            const StageArgs& a, int p, int k0, int i0, int j0) {
-  const int s = slot_of(p, k0);
-  if (p < 0 || p >= a.NZ) {
-    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&S.bar[s])) : "memory");
-    return;
-  }
-  mbar_expect_tx(&S.bar[s], kQBytes + kCBytes);
-  tma_load_4d(&S.slot[s].Q[0][0][0], tmQ, &S.bar[s], i0 - 4, j0 - 2, p, 0);
-  tma_load_3d(&S.slot[s].C[0][0], tmC, &S.bar[s], i0 - 16, j0 - 2, p);
-}
-
-// A wait ran out: flag the error for the host and wait (bounded) for the copies this CTA
-// still has in flight, so that none lands in shared memory after the CTA has left.
-__device__ void drain(TmaSmem& S, const StageArgs& a, int k0, int first_pending, int last_issued) {
-  if (threadIdx.x != 0) return;
-  atomicOr(a.err, 1);
-  for (int p = first_pending; p <= last_issued; p++) mbar_wait(&S.bar[slot_of(p, k0)], parity_of(p, k0));
-}
-
+// 80 registers without spills: three CTAs (24 warps) per SM.
 template <bool STAGE2>
-__global__ void __launch_bounds__(TX * TY, 2)
+__global__ void __launch_bounds__(TX * TY, 3)
     k_stage_tma(const __grid_constant__ CUtensorMap tmQ, const __grid_constant__ CUtensorMap tmC, StageArgs a,
                 int kz) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -380,13 +323,12 @@ int make_tensor_maps(a3d_solver* s) {
   CUresult r = enc(&s->tmC, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, s->code, cd, cs, cb, ce, CU_TENSOR_MAP_INTERLEAVE_NONE,
                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) { set_error("cuTensorMapEncodeTiled(codes) failed: %d", (int)r); return A3D_ERR_CUDA; }
-  static bool attr = false;
-  if (!attr) {
-    A3D_CUDA(cudaFuncSetAttribute(k_stage_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem_bytes()));
-    A3D_CUDA(cudaFuncSetAttribute(k_stage_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem_bytes()));
-    attr = true;
-  }
-  return A3D_OK;
+  // kernel attributes are per device: set them on every solver's device
+  A3D_CUDA(cudaFuncSetAttribute(k_stage_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem_bytes()));
+  A3D_CUDA(cudaFuncSetAttribute(k_stage_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem_bytes()));
+  A3D_CUDA(cudaFuncSetAttribute(k_stage_tma<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  A3D_CUDA(cudaFuncSetAttribute(k_stage_tma<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  return fused_set_attributes();
 }
 
 int launch_tma(a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2) {

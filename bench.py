@@ -32,6 +32,22 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 ALG_BYTES_PER_CELL_UPDATE = 142
+KERNEL_NAMES = {0: "k_stage_cell", 1: "k_stage_march", 2: "k_stage_tma", 3: "k_stage_fused"}
+
+
+def measured_traffic(kernel, cells):
+    """DRAM bytes per stage launch from the committed ncu summary (profiles/), scaled to `cells`.
+
+    The summary lists, per kernel, `traffic <kernel> <bytes per cell-stage>` measured as
+    dram__bytes_read.sum + dram__bytes_write.sum of single launches on the 4.13M-cell fighter."""
+    path = os.path.join(ROOT, "profiles", "stage_kernels_fighter4M.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        f = line.strip().strip("`").split()
+        if len(f) == 3 and f[0] == "traffic" and f[1] == kernel:
+            return float(f[2]) * cells
+    return None
 WORKLOAD = {"aircraft": "fighter", "cells": 4.0e6, "M": 0.6, "alpha": 3.0, "delta": 3.0, "iters": 2000}
 
 
@@ -43,10 +59,16 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--iters", type=int, default=WORKLOAD["iters"])
     p.add_argument("--cells", type=float, default=WORKLOAD["cells"])
-    p.add_argument("--kernel", type=int, default=1)
-    p.add_argument("--kz", type=int, default=16)
+    p.add_argument("--kernel", type=int, default=3)
+    p.add_argument("--kz", type=int, default=32)
     p.add_argument("--cpu-sample-iters", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--batch-cases", type=int, default=64)
+    p.add_argument("--batch-iters", type=int, default=1000)
+    p.add_argument("--serve-requests", type=int, default=32)
+    p.add_argument("--serve-rate", type=float, default=20.0)
+    p.add_argument("--no-batch", action="store_true")
+    p.add_argument("--no-serve", action="store_true")
     return p.parse_args()
 
 
@@ -155,6 +177,82 @@ def cpu_baseline(aero, sh, cells, iters, threads):
     return g.N * iters / dt, g.N
 
 
+def bench_batched(aero, args, ws, rank, local):
+    """C3: seeded cases of uneven size, all advanced together (one persistent launch per RK stage,
+    CUDA graph, autotuned schedule) vs the same cases solved one after another (plain loop).
+    The case list is sharded across ranks; solves/s are whole-job values (max time over ranks)."""
+    import torch
+    serve = importlib.import_module("3d_aero_lab_b200.serve")
+    reqs = serve.requests(1, args.batch_cases)[rank::ws]
+    cases = []
+    for r in reqs:
+        c = aero.Case(aircraft_type=r["type"], cells=r["cells"], M=r["M"], alpha=r["alpha"], delta=r["delta"],
+                      device=local)
+        cases.append(c)
+    cells = sum(c.g.N for c in cases)
+    it = args.batch_iters
+    # plain per-case loop
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain = []
+    for c in cases:
+        c.solver.reset()
+        c.solver.step(it)
+        plain.append(c.forces())
+    torch.cuda.synchronize()
+    t_plain = max_over_ranks(time.perf_counter() - t0, ws)
+    # batched
+    b = aero.Batch([c.solver for c in cases])
+    tuned = b.tune(4)
+    for c in cases:
+        c.solver.reset()
+    b.sync()
+    torch.cuda.synchronize()
+    barrier(ws)
+    t0 = time.perf_counter()
+    b.step(it)
+    b.sync()
+    batched = [c.forces() for c in cases]
+    t_batch = max_over_ranks(time.perf_counter() - t0, ws)
+    dcl = max(abs(x["CL"] - y["CL"]) for x, y in zip(plain, batched))
+    b.dispose()
+    for c in cases:
+        c.solver.dispose()
+    n = args.batch_cases
+    return {"workload": f"{n} cases (airliner/interceptor/fighter, 20k-2M cells, M 0.3-0.85, alpha -2..8, "
+                        f"delta -5..5, seed 1), {it} iterations each", "cells_per_rank": cells,
+            "solves_per_s": n / t_batch, "plain_loop_solves_per_s": n / t_plain, "speedup_vs_plain": t_plain / t_batch,
+            "cell_updates_per_s": ws * cells * it / t_batch, "schedule": tuned, "max_abs_dCL_batched_vs_plain": dcl}
+
+
+def bench_served(aero, args, ws, rank, local):
+    """C4: Poisson arrivals (seeded) of solve requests into the continuous-batching server, each
+    run to a 1e-3 density-residual drop or 3000 iterations, warm starts on repeated geometry,
+    150 GB admission budget; vs the same list solved one at a time in arrival order."""
+    serve = importlib.import_module("3d_aero_lab_b200.serve")
+    reqs = serve.requests(7, args.serve_requests, geometries=max(4, args.serve_requests // 3))[rank::ws]
+    sv = serve.Server(budget_gb=150.0, residual_drop=1e-3, max_active=64, chunk=50, max_iters=3000, device=local)
+    res, wall = serve.poisson_run(sv, reqs, args.serve_rate / ws, seed=7 + rank)
+    st = sv.stats()
+    sv.close()
+    lat = serve.latency_stats(res)
+    span = max(r["t_done"] for r in res) - min(r["t_submit"] for r in res)
+    plain, _ = serve.plain_loop(reqs, args.serve_rate / ws, seed=7 + rank)
+    plat = serve.latency_stats([dict(r, t_done=r["t_done"], t_submit=r["t_submit"]) for r in plain])
+    pspan = max(r["t_done"] for r in plain) - min(r["t_submit"] for r in plain)
+    span = max_over_ranks(span, ws)
+    pspan = max_over_ranks(pspan, ws)
+    dcl = max(abs(a["CL"] - b["CL"]) for a, b in zip(res, plain) if not a["warm"]) if any(not a["warm"] for a in res) else None
+    return {"workload": f"{args.serve_requests} requests, Poisson {args.serve_rate}/s (seed 7), C3 distribution with "
+                        f"{max(4, args.serve_requests // 3)} distinct geometries, residual drop 1e-3 or 3000 iterations",
+            "solves_per_s": args.serve_requests / span, "p50_s": lat["p50_s"], "p99_s": lat["p99_s"],
+            "plain_loop_solves_per_s": args.serve_requests / pspan, "plain_p50_s": plat["p50_s"],
+            "plain_p99_s": plat["p99_s"], "speedup_vs_plain": pspan / span,
+            "warm_starts": st["warm_starts"], "rounds": st["rounds"],
+            "mean_iterations": float(sum(r["iterations"] for r in res) / len(res)),
+            "max_abs_dCL_cold_vs_plain": dcl}
+
+
 def run_reference(args, ws, rank):
     """--impl reference: the reference's CPU algorithm (oracle port, all host threads)."""
     if rank != 0:
@@ -261,6 +359,18 @@ def main():
     t1.record(stream)
     t1.synchronize()
     e2e_ms = max_over_ranks(t0.elapsed_time(t1) / args.steps, ws)
+    s.dispose()
+    extra = {}
+    if not args.no_batch:
+        try:
+            extra["batched"] = bench_batched(aero, args, ws, rank, local)
+        except Exception as e:  # reported, not hidden
+            extra["batched"] = {"error": repr(e)}
+    if not args.no_serve:
+        try:
+            extra["served"] = bench_served(aero, args, ws, rank, local)
+        except Exception as e:
+            extra["served"] = {"error": repr(e)}
     cu = N * iters
     value = ws * cu / (ms * 1e-3)
     e2e = ws * cu / (e2e_ms * 1e-3)
@@ -280,20 +390,20 @@ def main():
                "config": {"workload": f"fighter plain solve, {g.NX}x{g.NY}x{g.NZ} = {N} cells, M0.6 a3 d3, "
                                       f"{iters} SSP-RK2 iterations per step",
                           "cells": N, "dims": [g.NX, g.NY, g.NZ], "iterations_per_step": iters,
-                          "kernel": "march" if args.kernel == 1 else "cell", "march_kz": args.kz,
+                          "kernel": {0: "cell", 1: "march", 2: "tma", 3: "fused"}[args.kernel], "march_kz": args.kz,
                           "l2": "inputs larger than L2 (three 5-component float32 states of %.0f MB each)"
                                 % (20 * N / 1e6),
                           "parallelism": f"{ws} independent solves (one per GPU)" if ws > 1 else "single GPU"},
                "e2e": {"value": e2e, "unit": "cell-updates/s", "h2d_bytes_per_step": 20 * N,
                        "d2h_bytes_per_step": 20 * N + 24},
                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                            "frac": achieved / peak, "traffic": None,
-                            "peak_source": peak_kind, "kernel": "k_stage_march" if args.kernel == 1 else "k_stage_cell",
+                            "frac": achieved / peak, "traffic": measured_traffic(KERNEL_NAMES[args.kernel], N),
+                            "peak_source": peak_kind, "kernel": KERNEL_NAMES[args.kernel],
                             "stage_ms": stage_ms},
                "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": launches_per_step * args.steps,
                "forces": {"CL": f["CL"], "CD": f["CD"], "Cm": f["Cm"], "CL_e2e": fe["CL"]}}
+        out.update(extra)
         print(json.dumps(out), flush=True)
-    s.dispose()
     if ws > 1:
         import torch.distributed as dist
         dist.barrier()

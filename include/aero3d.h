@@ -162,13 +162,86 @@ int a3d_solver_residual(a3d_solver* s, int32_t stride, double* res);
 int a3d_solver_mach_max(a3d_solver* s, int32_t stride, double* mmax);
 /* Stage kernel selection; no counterpart in the reference (it has one shader).
  * kernel 0: one thread per cell evaluating its six faces (the reference's structure);
- * kernel 1 (default): z-marching tiles that evaluate every face once; march_kz = z planes
- * per thread block.                                                                   */
+ * kernel 1: z-marching tiles that evaluate every face once, plain loads;
+ * kernel 2: the same fed by a TMA plane ring;
+ * kernel 3 (default): TMA ring, face states formed once per cell, paired f32x2 faces.
+ * march_kz = z planes per thread block (default 32).                                  */
 int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t march_kz);
 /* The solver's CUDA stream (a cudaStream_t), for callers that time or order work on it. */
 int a3d_solver_stream(a3d_solver* s, void** stream);
 /* Blocks until all work queued on the solver's stream has finished. */
 int a3d_solver_sync(a3d_solver* s);
+
+/* ---- batched solves: many cases in one persistent launch per RK stage ------------- */
+/* No counterpart in the reference (its controller runs one case).  A batch groups solver
+ * objects living on one device; a3d_batch_step(n) advances every case by n SSP-RK2
+ * iterations with one persistent kernel launch per stage (tiles of all cases pulled from a
+ * shared queue), two iterations captured once in a CUDA graph.  Each case keeps its own
+ * state, forces, residual and Trefftz calls; the batch orders itself after each solver's
+ * queued work and each solver's later work after the batch.                            */
+typedef struct a3d_batch a3d_batch;
+int a3d_batch_create(a3d_solver* const* solvers, int32_t n, a3d_batch** out);
+int a3d_batch_destroy(a3d_batch* b);
+int a3d_batch_step(a3d_batch* b, int32_t n);
+int a3d_batch_sync(a3d_batch* b);
+/* Tile schedule: z planes per tile (kz) and persistent CTAs per SM (1 or 2). */
+int a3d_batch_set_schedule(a3d_batch* b, int32_t kz, int32_t ctas_per_sm);
+int a3d_batch_get_schedule(a3d_batch* b, int32_t* kz, int32_t* ctas_per_sm, int64_t* tiles);
+/* Autotuner: times every (kz, CTAs per SM) candidate for trial_iters iterations on the real
+ * cases (states saved and restored), keeps the fastest; best_ms = ms per iteration.    */
+int a3d_batch_tune(a3d_batch* b, int32_t trial_iters, int32_t* best_kz, int32_t* best_ctas,
+                   float* best_ms);
+
+/* ---- continuous-batching solve server ----------------------------------------------- */
+/* No counterpart in the reference (its controller steps one case per animation frame).  A
+ * scheduler thread admits requests in arrival order while the estimated device memory of all
+ * resident cases fits `hbm_budget_bytes` and fewer than `max_active` run; every round advances
+ * all active cases by `chunk_iters` iterations in one batch (one persistent launch per RK
+ * stage), then checks each case's FP64 density residual (every fluid cell) against its first
+ * value.  A case finishes when the ratio is <= residual_drop or after max_iters iterations;
+ * its forces and Trefftz drag are computed on the device and it leaves the batch at once.
+ * With warm_start, finished cases stay resident keyed by `geometry_key` and a later request
+ * with the same key starts from that state (least recently used ones are evicted first).  */
+typedef struct a3d_server_config {
+  double hbm_budget_bytes;
+  double residual_drop;        /* e.g. 1e-3                                             */
+  int32_t max_active;          /* slot cap                                              */
+  int32_t chunk_iters;         /* iterations per round                                  */
+  int32_t max_iters;           /* iteration cap per request                             */
+  int32_t device;
+  int32_t warm_start;          /* 1: keep finished cases resident for reuse              */
+  int32_t kz;                  /* batch tile depth (z planes); 0: default               */
+} a3d_server_config;
+
+typedef struct a3d_request {
+  a3d_shape shape;
+  double cells, M, alpha_deg, delta_deg;
+  double F[5];                 /* far-field state (setFree)                              */
+  double fix[15];              /* fixed states of types 3, 4, 5 (setFix)                 */
+  double ref_S, ref_xcg, ref_zcg, ref_c;  /* force coefficients' reference values       */
+  double xT;                   /* Trefftz plane station                                  */
+  uint64_t geometry_key;       /* equal keys: same aircraft, cells and delta             */
+} a3d_request;
+
+typedef struct a3d_result {
+  int32_t status;              /* A3D_OK or the failing call's status                    */
+  int32_t warm;                /* 1: started from a resident converged state            */
+  int64_t iterations;
+  double CL, CD, Cm, CDi;
+  double residual, res0;       /* last and first density residual                       */
+  double t_submit, t_admit, t_done;  /* seconds on the server's clock                   */
+} a3d_result;
+
+typedef struct a3d_server a3d_server;
+int a3d_server_create(const a3d_server_config* cfg, a3d_server** out);
+/* Queues a request; A3D_ERR_BUDGET if it can never fit the budget. */
+int a3d_server_submit(a3d_server* sv, const a3d_request* req, int64_t* id);
+int a3d_server_poll(a3d_server* sv, int64_t id, a3d_result* out, int32_t* done);
+/* Waits up to timeout_s for a result (A3D_ERR_TIMEOUT otherwise). */
+int a3d_server_wait(a3d_server* sv, int64_t id, double timeout_s, a3d_result* out);
+/* pending, active, completed, warm starts, rounds, resident bytes */
+int a3d_server_stats(a3d_server* sv, int64_t out[6]);
+int a3d_server_destroy(a3d_server* sv);
 
 /* ---- force integral without device allocation ------------------------------------- */
 /* No counterpart in the reference.  The same C_L, C_D, C_m as a3d_solver_forces, for callers

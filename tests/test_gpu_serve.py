@@ -1,0 +1,50 @@
+"""Continuous-batching server: results in the mix equal results alone; warm starts; budget."""
+import importlib
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+REQS = [{"type": "fighter", "cells": 30000, "M": 0.6, "alpha": 3.0, "delta": 3.0},
+        {"type": "interceptor", "cells": 45000, "M": 0.8, "alpha": 1.0, "delta": -2.0},
+        {"type": "airliner", "cells": 60000, "M": 0.78, "alpha": 2.5, "delta": 0.0},
+        {"type": "fighter", "cells": 25000, "M": 0.45, "alpha": 6.0, "delta": 4.0}]
+KW = {"residual_drop": 0.1, "chunk": 25, "max_iters": 400}
+
+
+def test_results_in_the_mix_equal_results_alone(aero):
+    serve = importlib.import_module("3d_aero_lab_b200.serve")
+    sv = serve.Server(max_active=8, chunk=KW["chunk"], max_iters=KW["max_iters"], residual_drop=KW["residual_drop"],
+                      warm_start=False)
+    ids = [sv.submit(r) for r in REQS]           # all arrive together and overlap on the GPU
+    mixed = [sv.wait(i, 600) for i in ids]
+    st = sv.stats()
+    sv.close()
+    assert st["completed"] == len(REQS) and st["rounds"] < sum(m["iterations"] for m in mixed) / KW["chunk"]
+    for r, m in zip(REQS, mixed):
+        alone = serve.solve_plain(r, **KW)
+        assert m["status"] == 0 and m["iterations"] == alone["iterations"]
+        for k in ("CL", "CD", "Cm", "CDi"):
+            assert abs(m[k] - alone[k]) <= 1e-12 * max(1.0, abs(alone[k])), (r, k, m[k], alone[k])
+
+
+def test_warm_start_reuses_the_resident_case(aero):
+    serve = importlib.import_module("3d_aero_lab_b200.serve")
+    sv = serve.Server(max_active=4, chunk=KW["chunk"], max_iters=KW["max_iters"], residual_drop=KW["residual_drop"])
+    a = sv.wait(sv.submit(REQS[0]), 600)
+    b = sv.wait(sv.submit(REQS[0]), 600)  # same geometry and conditions: starts converged
+    st = sv.stats()
+    sv.close()
+    assert a["warm"] == 0 and b["warm"] == 1 and st["warm_starts"] == 1
+    assert b["res0"] == a["res0"] and b["iterations"] < a["iterations"]
+    assert abs(b["CL"] - a["CL"]) < 1e-3
+
+
+def test_request_beyond_the_budget_is_refused(aero):
+    serve = importlib.import_module("3d_aero_lab_b200.serve")
+    L = importlib.import_module("3d_aero_lab_b200._lib")
+    sv = serve.Server(budget_gb=0.5, max_active=2)
+    with pytest.raises(L.AeroError) as e:
+        sv.submit(dict(REQS[0], cells=2.0e7))
+    assert e.value.status == 6
+    sv.close()

@@ -39,7 +39,7 @@ def sig4(x):
     return float(f"{x:.4g}")
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 2])
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3])
 def test_readme_case_matches_oracle_and_pin(aero, ref, kernel):
     ac, sh, og, ogeo, o = oracle_case(aero, ref, "fighter", 30000, 3.0)
     g, s = gpu_case(aero, sh, 30000, 3.0, kernel=kernel)
@@ -57,7 +57,7 @@ def test_readme_case_matches_oracle_and_pin(aero, ref, kernel):
     assert round(fg["CL"], 4) == README_CL and round(fg["CD"], 5) == README_CD
 
 
-@pytest.mark.parametrize("kernel", [1, 2])
+@pytest.mark.parametrize("kernel", [1, 2, 3])
 def test_kernels_agree(aero, kernel):
     """The tiled kernels against the per-cell one (same float32 arithmetic, other summation order)."""
     sh = aero.shape_of(aero.build_aircraft("airliner"))
@@ -71,7 +71,7 @@ def test_kernels_agree(aero, kernel):
 
 @pytest.mark.parametrize("seed,dims,order", [(0, (9, 7, 6), 2), (1, (33, 9, 20), 2), (2, (40, 17, 3), 1),
                                              (3, (5, 2, 35), 2), (4, (64, 12, 18), 2)])
-@pytest.mark.parametrize("kernel", [0, 1, 2])
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3])
 def test_random_boxes_per_cell(aero, ref, seed, dims, order, kernel):
     """Random cut cells, solids, fixed cells and baffles; every cell after 1 and 15 iterations."""
     rng = np.random.default_rng(seed)
