@@ -59,10 +59,10 @@ struct a3d_solver {
   double cfl = 0.7;
   int order = 2;
   long it = 0;
-  int kernel = a3d::KERNEL_FUSED;
+  int kernel = a3d::KERNEL_TMA;      // fastest single-case stage kernel on B200
   CUtensorMap tmQ[3];             // TMA maps over the three state buffers
   CUtensorMap tmC;                // TMA map over the code array
-  int march_kz = 32;              // z planes per CTA of the marching kernels
+  int march_kz = 16;              // z planes per CTA of the marching kernels
   // reductions
   double* d_red = nullptr;        // device partials + results
   double* h_red = nullptr;        // pinned host mirror of the results

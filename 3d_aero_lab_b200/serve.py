@@ -139,11 +139,13 @@ def latency_stats(res):
             "mean_s": float(lat.mean()), "max_s": float(lat.max())}
 
 
-def solve_plain(r, residual_drop=1e-3, chunk=50, max_iters=3000, device=0):
-    """One request on its own solver, the same convergence rule as the server."""
+def solve_plain(r, residual_drop=1e-3, chunk=50, max_iters=3000, device=0, kernel=3):
+    """One request on its own solver, the same convergence rule as the server.  Kernel 3 is
+    the tile the server's batches run, so the two give bit-identical results."""
     ac, sh = aircraft(r["type"])
     g = cfd_grid(sh, r["cells"])
     s = CfdGPU(g, shape=sh, delta=r["delta"], device=device)
+    s.set_kernel(kernel, 16)
     F = freestream(r["M"], r["alpha"])
     s.setFree(F)
     s.setFix([F, F, F])

@@ -163,9 +163,10 @@ int a3d_solver_mach_max(a3d_solver* s, int32_t stride, double* mmax);
 /* Stage kernel selection; no counterpart in the reference (it has one shader).
  * kernel 0: one thread per cell evaluating its six faces (the reference's structure);
  * kernel 1: z-marching tiles that evaluate every face once, plain loads;
- * kernel 2: the same fed by a TMA plane ring;
- * kernel 3 (default): TMA ring, face states formed once per cell, paired f32x2 faces.
- * march_kz = z planes per thread block (default 32).                                  */
+ * kernel 2 (default): the same fed by a TMA plane ring, three CTAs per SM;
+ * kernel 3: TMA ring, face states formed once per cell, paired f32x2 faces; results do
+ *           not depend on the tiling, and the batch and server paths use this tile.
+ * march_kz = z planes per thread block (default 16).                                  */
 int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t march_kz);
 /* The solver's CUDA stream (a cudaStream_t), for callers that time or order work on it. */
 int a3d_solver_stream(a3d_solver* s, void** stream);
