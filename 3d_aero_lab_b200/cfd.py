@@ -227,6 +227,14 @@ class CfdGPU:
         _lib.check(_lib.lib().a3d_solver_residual(self._h, int(stride), C.byref(v)))
         return None if v.value < 0 else v.value
 
+    def sample(self, xyz):
+        """Primitive states at points (n x 3): (n x 5 array, ok flags) - cfdStencil + cfdSample."""
+        xyz = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)
+        out = np.zeros((len(xyz), 5))
+        ok = np.zeros(len(xyz), np.int32)
+        _lib.check(_lib.lib().a3d_solver_sample(self._h, len(xyz), xyz.reshape(-1), out.reshape(-1), ok))
+        return out, ok.astype(bool)
+
     def mach_max(self, stride=2):
         v = C.c_double()
         _lib.check(_lib.lib().a3d_solver_mach_max(self._h, int(stride), C.byref(v)))

@@ -39,7 +39,8 @@ def measured_traffic(kernel, cells):
     """DRAM bytes per stage launch from the committed ncu summary (profiles/), scaled to `cells`.
 
     The summary lists, per kernel, `traffic <kernel> <bytes per cell-stage>` measured as
-    dram__bytes_read.sum + dram__bytes_write.sum of single launches on the 4.13M-cell fighter."""
+    dram__bytes_read.sum + dram__bytes_write.sum of single launches on the 4.13M-cell fighter
+    (mean of a stage-1 and a stage-2 launch)."""
     path = os.path.join(ROOT, "profiles", "stage_kernels_fighter4M.md")
     if not os.path.exists(path):
         return None
@@ -59,6 +60,10 @@ def parse():
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--iters", type=int, default=WORKLOAD["iters"])
     p.add_argument("--cells", type=float, default=WORKLOAD["cells"])
+    p.add_argument("--aircraft", default=WORKLOAD["aircraft"], choices=["fighter", "interceptor", "airliner"])
+    p.add_argument("--mach", type=float, default=WORKLOAD["M"])
+    p.add_argument("--alpha", type=float, default=WORKLOAD["alpha"])
+    p.add_argument("--delta", type=float, default=WORKLOAD["delta"])
     p.add_argument("--kernel", type=int, default=2)
     p.add_argument("--kz", type=int, default=16)
     p.add_argument("--cpu-sample-iters", type=int, default=2)
@@ -159,14 +164,14 @@ def barrier(ws):
         dist.barrier()
 
 
-def cpu_baseline(aero, sh, cells, iters, threads):
+def cpu_baseline(aero, sh, cells, iters, threads, M, alpha, delta):
     """The oracle (C++ CfdCPU restatement, f32 storage / f64 arithmetic) on a bounded sample."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref
     g = ref.grid(sh, cells)
-    geo = ref.geom(sh, g, WORKLOAD["delta"])
+    geo = ref.geom(sh, g, delta)
     s = ref.CfdCPU(g, geo, threads=threads)
-    F = aero.cfd.freestream(WORKLOAD["M"], WORKLOAD["alpha"])
+    F = aero.cfd.freestream(M, alpha)
     s.setFree(F)
     s.setFix([F, F, F])
     s.reset()
@@ -300,10 +305,10 @@ def main():
     import torch
     aero = importlib.import_module("3d_aero_lab_b200")
     torch.cuda.set_device(local)
-    alpha = WORKLOAD["alpha"] + 0.25 * rank  # independent case per rank
-    ac = aero.build_aircraft(WORKLOAD["aircraft"])
+    alpha = args.alpha + 0.25 * rank  # independent case per rank
+    ac = aero.build_aircraft(args.aircraft)
     sh = aero.shape_of(ac)
-    case = aero.Case(ac=ac, cells=args.cells, M=WORKLOAD["M"], alpha=alpha, delta=WORKLOAD["delta"], device=local)
+    case = aero.Case(ac=ac, cells=args.cells, M=args.mach, alpha=alpha, delta=args.delta, device=local)
     s = case.solver
     s.set_kernel(args.kernel, args.kz)
     g = case.g
@@ -381,15 +386,15 @@ def main():
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline and ws == 1:
-            v, n_cpu = cpu_baseline(aero, sh, args.cells, args.cpu_sample_iters, 1)
+            v, n_cpu = cpu_baseline(aero, sh, args.cells, args.cpu_sample_iters, 1, args.mach, args.alpha, args.delta)
             cpu = {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": "port",
                    "sample": f"{args.cpu_sample_iters} iterations of the same {g.NX}x{g.NY}x{g.NZ} grid, 1 thread "
                              "(C++ restatement of CfdCPU; the JavaScript original cannot run here)"}
         out = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": ws,
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-               "config": {"workload": f"fighter plain solve, {g.NX}x{g.NY}x{g.NZ} = {N} cells, M0.6 a3 d3, "
-                                      f"{iters} SSP-RK2 iterations per step",
+               "config": {"workload": f"{args.aircraft} plain solve, {g.NX}x{g.NY}x{g.NZ} = {N} cells, "
+                                      f"M{args.mach} a{args.alpha} d{args.delta}, {iters} SSP-RK2 iterations per step",
                           "cells": N, "dims": [g.NX, g.NY, g.NZ], "iterations_per_step": iters,
                           "kernel": {0: "cell", 1: "march", 2: "tma", 3: "fused"}[args.kernel], "march_kz": args.kz,
                           "l2": "inputs larger than L2 (three 5-component float32 states of %.0f MB each)"

@@ -160,6 +160,10 @@ int a3d_solver_trefftz(a3d_solver* s, double xT, double alpha_deg, double M, dou
 int a3d_solver_residual(a3d_solver* s, int32_t stride, double* res);
 /* Largest Mach number over fluid cells with q % stride == 0 (src/air_cfd.js:571). */
 int a3d_solver_mach_max(a3d_solver* s, int32_t stride, double* mmax);
+/* Display sampling cfdStencil + cfdSample (src/air_cfd.js:455-482) on the device: primitive
+ * states (rho, u, v, w, p) at n points xyz (FP64, x/y/z interleaved), so that surfaces,
+ * slices and probes need no full read().  ok[p] = 0 where no fluid cell is near.        */
+int a3d_solver_sample(a3d_solver* s, int32_t n, const double* xyz, double* out5, int32_t* ok);
 /* Stage kernel selection; no counterpart in the reference (it has one shader).
  * kernel 0: one thread per cell evaluating its six faces (the reference's structure);
  * kernel 1: z-marching tiles that evaluate every face once, plain loads;

@@ -699,3 +699,53 @@ int ref_max_threads(void) {
 
 extern "C" void ref_hllc(const double* L, const double* R, int d, double* out) { cfdHLLC(L, R, d, out); }
 extern "C" void ref_prim(const double* U, double* P) { cfdPrim5(U[0], U[1], U[2], U[3], U[4], P); }
+
+/* ---- display sampling: cfdStencil + cfdSample (src/air_cfd.js:453-482) ---- */
+namespace {
+template <typename ST>
+int sample_one(const RefSolver<ST>& s, double x, double y, double z, double* out) {
+  const Grid& G = s.G;
+  int i, j, k; double tx, ty, tz;
+  cfdLocate(G.Xc, x, i, tx); cfdLocate(G.Yc, std::fabs(y), j, ty); cfdLocate(G.Zc, z, k, tz);
+  long idx[8]; double w[8]; double ws = 0;
+  for (int c = 0; c < 8; c++) {
+    const int di = c & 1, dj = (c >> 1) & 1, dk = c >> 2;
+    const long q = ((long)(k + dk) * G.NY + (j + dj)) * G.NX + (i + di);
+    const double ww = (di ? tx : 1 - tx) * (dj ? ty : 1 - ty) * (dk ? tz : 1 - tz);
+    const bool ok = s.t[q] == 0 || s.t[q] >= 3;
+    idx[c] = q; w[c] = ok ? ww : 0; ws += ok ? ww : 0;
+  }
+  if (ws > 1e-6) { for (int c = 0; c < 8; c++) w[c] /= ws; }
+  else {
+    long best = -1; double bd = INFINITY;
+    for (int dk = -1; dk <= 2; dk++) for (int dj = -1; dj <= 2; dj++) for (int di = -1; di <= 2; di++) {
+      const int a = i + di, b = j + dj, c = k + dk;
+      if (a < 0 || b < 0 || c < 0 || a >= G.NX || b >= G.NY || c >= G.NZ) continue;
+      const long q = ((long)c * G.NY + b) * G.NX + a;
+      if (s.t[q] != 0) continue;
+      const double d2 = std::pow((double)G.Xc[a] - x, 2) + std::pow((double)G.Yc[b] - std::fabs(y), 2) + std::pow((double)G.Zc[c] - z, 2);
+      if (d2 < bd) { bd = d2; best = q; }
+    }
+    for (int c = 0; c < 8; c++) { idx[c] = best < 0 ? 0 : best; w[c] = best < 0 ? 0 : (c == 0 ? 1 : 0); }
+  }
+  double r = 0, ru = 0, rv = 0, rw = 0, E = 0, wsum = 0;
+  for (int c = 0; c < 8; c++) {
+    const double ww = w[c];
+    if (!(ww != 0)) continue;
+    const long q = idx[c];
+    r += ww * (double)s.Q[0][q]; ru += ww * (double)s.Q[1][q]; rv += ww * (double)s.Q[2][q];
+    rw += ww * (double)s.Q[3][q]; E += ww * (double)s.Q[4][q]; wsum += ww;
+  }
+  if (wsum == 0) return 0;
+  const double ysgn = y < 0 ? -1 : 1;
+  r = std::max(r, 1e-6);
+  const double u = ru / r, v = rv / r * ysgn, wv = rw / r;
+  out[0] = r; out[1] = u; out[2] = v; out[3] = wv;
+  out[4] = std::max((CG - 1) * (E - 0.5 * r * (u * u + v * v + wv * wv)), 1e-7);
+  return 1;
+}
+}  // namespace
+
+extern "C" void ref_solver_sample(void* h, int n, const double* xyz, double* out5, int* ok) {
+  DISPATCH(h, for (int p = 0; p < n; p++) ok[p] = sample_one(*S_, xyz[3 * p], xyz[3 * p + 1], xyz[3 * p + 2], out5 + 5 * p));
+}

@@ -194,3 +194,15 @@ def prim(U):
     out = np.zeros(5)
     lb.ref_prim(np.asarray(U, np.float64), out)
     return out
+
+
+def sample(solver, xyz):
+    """cfdStencil + cfdSample of the oracle at points xyz (n x 3): (n x 5 primitives, ok flags)."""
+    lb = lib()
+    lb.ref_solver_sample.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _i32]
+    lb.ref_solver_sample.restype = None
+    xyz = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)
+    out = np.zeros((len(xyz), 5))
+    ok = np.zeros(len(xyz), np.int32)
+    lb.ref_solver_sample(solver._h, len(xyz), xyz.reshape(-1), out.reshape(-1), ok)
+    return out, ok.astype(bool)

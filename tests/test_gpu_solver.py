@@ -150,3 +150,21 @@ def test_nonfinite_state_is_reported(aero):
     with pytest.raises(L.AeroError) as e:
         s.residual(3)
     assert e.value.status == 4
+
+
+def test_display_sampling_matches_oracle(aero, ref):
+    """cfdStencil + cfdSample on the device vs the oracle, on the same state (FP64 both)."""
+    ac, sh, og, ogeo, o = oracle_case(aero, ref, "airliner", 150000, 2.0, M=0.78, alpha=2.5)
+    g, s = gpu_case(aero, sh, 150000, 2.0, M=0.78, alpha=2.5)
+    o.step(20)
+    s.write(o.read().astype(np.float32))
+    rng = np.random.default_rng(3)
+    lo = np.array([og.xf[0], -og.yf[-1], og.zf[0]])
+    hi = np.array([og.xf[-1], og.yf[-1], og.zf[-1]])
+    pts = lo + (hi - lo) * rng.random((4000, 3))
+    near = np.array([[ac.fus.L * f, 0.3 * ac.fus.R0, 0.0] for f in np.linspace(0, 1, 200)])  # hug the body
+    pts = np.vstack([pts, near, [[-1e3, 0, 0], [1e3, 1e3, 1e3]]])
+    a, oka = s.sample(pts)
+    b, okb = ref.sample(o, pts)
+    assert np.array_equal(oka, okb) and oka.sum() > 4000
+    assert np.allclose(a[oka], b[okb], rtol=1e-12, atol=1e-14)
