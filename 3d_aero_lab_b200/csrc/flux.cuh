@@ -42,9 +42,9 @@ __device__ __forceinline__ Prim rot(const float P[5], int d) {
 // HLLC flux with Davis wave-speed estimates (cfdHLLC, src/air_cfd.js:179-195).
 // Output: mass, normal momentum, tangential momenta, energy.
 __device__ __forceinline__ void hllc(const Prim& L, const Prim& R, float F[5]) {
-  const float aL = sqrtf(kG * L.p / L.r), aR = sqrtf(kG * R.p / R.r);
-  const float EL = L.p / kGm + 0.5f * L.r * (L.un * L.un + L.u1 * L.u1 + L.u2 * L.u2);
-  const float ER = R.p / kGm + 0.5f * R.r * (R.un * R.un + R.u1 * R.u1 + R.u2 * R.u2);
+  const float aL = sqrtf(__fdividef(kG * L.p, L.r)), aR = sqrtf(__fdividef(kG * R.p, R.r));
+  const float EL = L.p * (1.0f / kGm) + 0.5f * L.r * (L.un * L.un + L.u1 * L.u1 + L.u2 * L.u2);
+  const float ER = R.p * (1.0f / kGm) + 0.5f * R.r * (R.un * R.un + R.u1 * R.u1 + R.u2 * R.u2);
   const float SL = fminf(L.un - aL, R.un - aR), SR = fmaxf(L.un + aL, R.un + aR);
   if (SL >= 0.f || SR <= 0.f) {  // supersonic: upwind state flux
     const bool left = SL >= 0.f;
@@ -53,18 +53,18 @@ __device__ __forceinline__ void hllc(const Prim& L, const Prim& R, float F[5]) {
     F[0] = m; F[1] = m * K.un + K.p; F[2] = m * K.u1; F[3] = m * K.u2; F[4] = K.un * (E + K.p);
     return;
   }
-  const float SM = (R.p - L.p + L.r * L.un * (SL - L.un) - R.r * R.un * (SR - R.un)) /
-                   (L.r * (SL - L.un) - R.r * (SR - R.un));
+  const float SM = __fdividef(R.p - L.p + L.r * L.un * (SL - L.un) - R.r * R.un * (SR - R.un),
+                              L.r * (SL - L.un) - R.r * (SR - R.un));
   const bool left = SM >= 0.f;
   const float rK = left ? L.r : R.r, uK = left ? L.un : R.un, v1 = left ? L.u1 : R.u1, v2 = left ? L.u2 : R.u2;
   const float pK = left ? L.p : R.p, EK = left ? EL : ER, S = left ? SL : SR;
-  const float f = rK * (S - uK) / (S - SM);
+  const float f = __fdividef(rK * (S - uK), S - SM);
   const float m = rK * uK;
   F[0] = m + S * (f - rK);
   F[1] = m * uK + pK + S * (f * SM - m);
   F[2] = m * v1 + S * (f * v1 - rK * v1);
   F[3] = m * v2 + S * (f * v2 - rK * v2);
-  const float Es = f * (EK / rK + (SM - uK) * (SM + pK / (rK * (S - uK))));
+  const float Es = f * (__fdividef(EK, rK) + (SM - uK) * (SM + __fdividef(pK, rK * (S - uK))));
   F[4] = uK * (EK + pK) + S * (Es - EK);
 }
 
