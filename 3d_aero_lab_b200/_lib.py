@@ -56,6 +56,7 @@ PROTOS = {
     "a3d_solver_set_kernel": (C.c_int, [_vp, C.c_int32, C.c_int32]),
     "a3d_solver_stream": (C.c_int, [_vp, C.POINTER(_vp)]),
     "a3d_solver_sample": (C.c_int, [_vp, C.c_int32, _dp, _dp, _i32]),
+    "a3d_solver_interp_state": (C.c_int, [_vp, _vp]),
     "a3d_solver_sync": (C.c_int, [_vp]),
     "a3d_batch_create": (C.c_int, [C.POINTER(_vp), C.c_int32, C.POINTER(_vp)]),
     "a3d_batch_destroy": (C.c_int, [_vp]),

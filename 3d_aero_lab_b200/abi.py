@@ -40,7 +40,8 @@ class a3d_shape(C.Structure):
 class a3d_server_config(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_double), ("residual_drop", C.c_double), ("max_active", C.c_int32),
                 ("chunk_iters", C.c_int32), ("max_iters", C.c_int32), ("device", C.c_int32),
-                ("warm_start", C.c_int32), ("kz", C.c_int32)]
+                ("warm_start", C.c_int32), ("kz", C.c_int32), ("sequence", C.c_int32),
+                ("sequence_max_iters", C.c_int32), ("sequence_drop", C.c_double)]
 
 
 class a3d_request(C.Structure):
@@ -54,4 +55,5 @@ class a3d_result(C.Structure):
     _fields_ = [("status", C.c_int32), ("warm", C.c_int32), ("iterations", C.c_int64),
                 ("CL", C.c_double), ("CD", C.c_double), ("Cm", C.c_double), ("CDi", C.c_double),
                 ("residual", C.c_double), ("res0", C.c_double),
-                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double)]
+                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_done", C.c_double),
+                ("coarse_iterations", C.c_int64)]

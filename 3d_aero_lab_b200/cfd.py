@@ -235,10 +235,20 @@ class CfdGPU:
         _lib.check(_lib.lib().a3d_solver_sample(self._h, len(xyz), xyz.reshape(-1), out.reshape(-1), ok))
         return out, ok.astype(bool)
 
+    def interp_from(self, coarse):
+        """Start from `coarse`'s state interpolated onto this grid (interpState, grid sequencing)."""
+        _lib.check(_lib.lib().a3d_solver_interp_state(self._h, coarse._h))
+
     def mach_max(self, stride=2):
         v = C.c_double()
         _lib.check(_lib.lib().a3d_solver_mach_max(self._h, int(stride), C.byref(v)))
         return v.value
+
+
+def interp_state(coarse, fine):
+    """interpState (src/app_cfd.js:331-357) in 3-D: `fine` takes `coarse`'s state on its cells."""
+    fine.interp_from(coarse)
+    return fine
 
 
 class Case:

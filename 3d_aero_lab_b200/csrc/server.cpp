@@ -11,7 +11,12 @@
 //     (one persistent launch per RK stage, batch.cu), then checks each case's FP64 density
 //     residual (src/air_cfd.js:552-555, every fluid cell) against its first one;
 //   * a case that dropped by the configured ratio or reached the iteration cap gets its FP64
-//     forces and Trefftz drag and leaves; the next round already contains the newcomers.
+//     forces and Trefftz drag and leaves; the next round already contains the newcomers;
+//   * grid sequencing (src/app_cfd.js:271-278, 398-403), when configured: a cold request first
+//     runs a coarse case of the same geometry in the batch; when that has dropped its residual
+//     (or hit its cap) the requested case measures its own free-stream res0 over one chunk,
+//     takes the coarse state interpolated onto its cells (interp.cu) and carries on in the
+//     batch in the coarse case's place.
 // Each case's arithmetic is the same in the mix as alone: the batched tile is the single-case
 // tile, and every case checks its residual every `chunk` of its own iterations.
 #include <chrono>
@@ -38,6 +43,10 @@ struct Job {
   long it_start = 0;
   bool done = false;
   size_t bytes = 0;
+  a3d_solver* coarse = nullptr;  // grid sequencing: the coarse case while it runs
+  size_t coarse_bytes = 0;
+  double coarse_res0 = -1;
+  long coarse_its = 0;
 };
 
 struct Cached {
@@ -50,6 +59,13 @@ struct Cached {
 size_t case_bytes(const int32_t dims[3]) {
   const double N = (double)dims[0] * dims[1] * dims[2];
   return (size_t)(N * 96.0) + (64u << 20);  // 3 x 20 B state, 21 B geometry, codes, snapshot, scratch
+}
+
+// Admission estimate of a request before its grid exists (target cells, plus the coarse case).
+double request_bytes(const a3d_request& r, int sequence) {
+  double b = r.cells * 96.0 + (64u << 20);
+  if (sequence > 1) b += r.cells / sequence * 96.0 + (64u << 20);
+  return b;
 }
 
 }  // namespace
@@ -89,6 +105,56 @@ void make_room(a3d_server* sv, size_t need) {
   }
 }
 
+// The coarse case of a sequenced request: cells / sequence, same shape and delta, free stream.
+int start_coarse(a3d_server* sv, Job& j) {
+  const a3d_request& r = j.req;
+  std::vector<double> xf(16384), yf(16384), zf(16384);
+  int32_t dims[3];
+  double h, core[5];
+  int rc = a3d_grid_build(&r.shape, r.cells / sv->cfg.sequence, 16384, xf.data(), yf.data(), zf.data(), dims, &h,
+                          core);
+  if (rc != A3D_OK) return rc;
+  if (dims[0] < 2 || dims[1] < 2 || dims[2] < 2) return A3D_OK;  // nothing to interpolate from: no sequencing
+  const size_t bytes = case_bytes(dims);
+  make_room(sv, bytes);
+  rc = a3d_solver_create_shape(&r.shape, dims, xf.data(), yf.data(), zf.data(), h, r.delta_deg, sv->cfg.device,
+                               &j.coarse);
+  if (rc != A3D_OK) return rc;
+  sv->resident += bytes;
+  j.coarse_bytes = bytes;
+  a3d_solver_set_free(j.coarse, r.F);
+  a3d_solver_set_fix(j.coarse, r.fix);
+  a3d_solver_reset(j.coarse);
+  double dummy;
+  return a3d_solver_residual(j.coarse, 1, &dummy);  // snapshot
+}
+
+void drop_coarse(a3d_server* sv, Job& j) {
+  if (!j.coarse) return;
+  a3d_solver_destroy(j.coarse);
+  sv->resident -= j.coarse_bytes;
+  j.coarse = nullptr;
+  j.coarse_bytes = 0;
+}
+
+// Coarse case done: the requested case measures its free-stream res0 over one chunk (on the
+// batch tile kernel, so the value is the one a cold batched run gets), then starts from the
+// coarse state.  The probe chunk counts towards the case's iterations.
+int switch_to_target(a3d_server* sv, Job& j) {
+  j.coarse_its = j.coarse->it;
+  const int chunk = sv->cfg.chunk_iters;
+  int rc = a3d_solver_set_kernel(j.s, a3d::KERNEL_FUSED, sv->cfg.kz);
+  if (rc == A3D_OK) rc = a3d_solver_step(j.s, chunk);
+  double r0 = -1, dummy;
+  if (rc == A3D_OK) rc = a3d_solver_residual(j.s, 1, &r0);
+  if (rc == A3D_OK) j.res0 = r0;
+  if (rc == A3D_OK) rc = a3d_solver_interp_state(j.s, j.coarse);
+  if (rc == A3D_OK) rc = a3d_solver_residual(j.s, 1, &dummy);  // snapshot of the interpolated start
+  drop_coarse(sv, j);
+  j.it_start = j.s->it - chunk;
+  return rc;
+}
+
 int start_case(a3d_server* sv, Job& j) {
   const a3d_request& r = j.req;
   std::vector<double> xf(16384), yf(16384), zf(16384);
@@ -117,6 +183,7 @@ int start_case(a3d_server* sv, Job& j) {
   j.it_start = j.s->it;
   double dummy;
   a3d_solver_residual(j.s, 1, &dummy);  // snapshot
+  if (!j.res.warm && sv->cfg.sequence > 1) return start_coarse(sv, j);
   return A3D_OK;
 }
 
@@ -133,6 +200,8 @@ void finish_case(a3d_server* sv, Job& j, int status) {
     o.status = rc;
   }
   o.res0 = j.res0;
+  o.coarse_iterations = j.coarse_its;
+  drop_coarse(sv, j);
   j.t_done = Clock::now();
   o.t_submit = secs(sv, j.t_submit);
   o.t_admit = secs(sv, j.t_admit);
@@ -165,7 +234,7 @@ void scheduler(a3d_server* sv) {
       size_t planned = sv->resident;
       while (!sv->pending.empty() && (int)(sv->active.size() + admit.size()) < sv->cfg.max_active) {
         auto& j = sv->pending.front();
-        const double est = j->req.cells * 96.0 + (64u << 20);
+        const double est = request_bytes(j->req, sv->cfg.sequence);
         const bool warm = sv->cfg.warm_start && sv->cache.count(j->req.geometry_key);
         size_t idle = 0;
         for (auto& c : sv->cache) idle += c.second.bytes;
@@ -194,7 +263,7 @@ void scheduler(a3d_server* sv) {
     if (act.empty()) continue;
     // one round: all active cases advance together
     std::vector<a3d_solver*> set;
-    for (auto& j : act) set.push_back(j->s);
+    for (auto& j : act) set.push_back(j->coarse ? j->coarse : j->s);
     if (set != batch_set) {
       if (batch) a3d_batch_destroy(batch);
       batch = nullptr;
@@ -217,7 +286,19 @@ void scheduler(a3d_server* sv) {
     std::vector<std::shared_ptr<Job>> still;
     for (auto& j : act) {
       double res = -1;
-      int st = rc != A3D_OK ? rc : a3d_solver_residual(j->s, 1, &res);
+      int st = rc != A3D_OK ? rc : a3d_solver_residual(j->coarse ? j->coarse : j->s, 1, &res);
+      if (st == A3D_OK && j->coarse) {  // sequencing: the coarse case's own stopping rule
+        if (j->coarse_res0 <= 0 && res > 0) j->coarse_res0 = res;
+        if ((j->coarse_res0 > 0 && res / j->coarse_res0 <= sv->cfg.sequence_drop) ||
+            j->coarse->it >= sv->cfg.sequence_max_iters) {
+          std::lock_guard<std::mutex> lk(sv->mu);
+          st = switch_to_target(sv, *j);
+        }
+        if (st == A3D_OK) {
+          still.push_back(j);
+          continue;
+        }
+      }
       const long its = j->s->it - j->it_start;
       bool fin = st != A3D_OK;
       if (!fin) {
@@ -250,6 +331,7 @@ extern "C" int a3d_server_create(const a3d_server_config* cfg, a3d_server** out)
   A3D_ARG(cfg && out, "null pointer");
   A3D_ARG(cfg->chunk_iters >= 1 && cfg->max_iters >= 1 && cfg->max_active >= 1, "server limits");
   A3D_ARG(cfg->hbm_budget_bytes > 0 && cfg->residual_drop > 0, "server budget / residual drop");
+  A3D_ARG(cfg->sequence <= 1 || (cfg->sequence_drop > 0 && cfg->sequence_max_iters >= 1), "sequencing limits");
   A3D_TRY(use_device(cfg->device));
   a3d_server* sv = new a3d_server();
   sv->cfg = *cfg;
@@ -269,8 +351,9 @@ extern "C" int a3d_server_submit(a3d_server* sv, const a3d_request* req, int64_t
   j->t_submit = Clock::now();
   {
     std::lock_guard<std::mutex> lk(sv->mu);
-    if (req->cells * 96.0 > sv->cfg.hbm_budget_bytes) {
-      set_error("request needs about %.1f GB, above the %.1f GB budget", req->cells * 96e-9, sv->cfg.hbm_budget_bytes * 1e-9);
+    if (request_bytes(*req, sv->cfg.sequence) > sv->cfg.hbm_budget_bytes) {
+      set_error("request needs about %.1f GB, above the %.1f GB budget", request_bytes(*req, sv->cfg.sequence) * 1e-9,
+                sv->cfg.hbm_budget_bytes * 1e-9);
       return A3D_ERR_BUDGET;
     }
     j->id = sv->next_id++;

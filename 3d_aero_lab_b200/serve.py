@@ -74,9 +74,11 @@ def result_dict(o):
 
 class Server:
     def __init__(self, budget_gb=150.0, residual_drop=1e-3, max_active=64, chunk=50, max_iters=3000, device=0,
-                 warm_start=True, kz=16):
+                 warm_start=True, kz=16, sequence=0, sequence_drop=0.05, sequence_max_iters=1500):
+        """sequence: grid sequencing factor (a cold request first solves cells/sequence cells,
+        until its residual dropped by sequence_drop or sequence_max_iters; 0 = off)."""
         cfg = a3d_server_config(budget_gb * 1e9, residual_drop, max_active, chunk, max_iters, device,
-                                1 if warm_start else 0, kz)
+                                1 if warm_start else 0, kz, sequence, sequence_max_iters, sequence_drop)
         self._h = C.c_void_p()
         _lib.check(_lib.lib().a3d_server_create(C.byref(cfg), C.byref(self._h)))
 

@@ -72,6 +72,7 @@ def parse():
     p.add_argument("--batch-iters", type=int, default=1000)
     p.add_argument("--serve-requests", type=int, default=32)
     p.add_argument("--serve-rate", type=float, default=20.0)
+    p.add_argument("--serve-sequence", type=int, default=8)
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--no-serve", action="store_true")
     return p.parse_args()
@@ -243,6 +244,20 @@ def bench_served(aero, args, ws, rank, local):
     sv.close()
     lat = serve.latency_stats(res)
     span = max(r["t_done"] for r in res) - min(r["t_submit"] for r in res)
+    seq = None
+    if args.serve_sequence > 1:  # the same arrivals with grid sequencing (coarse case at cells/8 first)
+        sq = serve.Server(budget_gb=150.0, residual_drop=1e-3, max_active=64, chunk=50, max_iters=3000, device=local,
+                          sequence=args.serve_sequence, sequence_drop=0.05, sequence_max_iters=1500)
+        sres, _ = serve.poisson_run(sq, reqs, args.serve_rate / ws, seed=7 + rank)
+        sq.close()
+        slat = serve.latency_stats(sres)
+        sspan = max_over_ranks(max(r["t_done"] for r in sres) - min(r["t_submit"] for r in sres), ws)
+        cold = [(a, b) for a, b in zip(res, sres) if not a["warm"] and not b["warm"]]
+        seq = {"sequence": args.serve_sequence, "solves_per_s": args.serve_requests / sspan, "p50_s": slat["p50_s"],
+               "p99_s": slat["p99_s"], "mean_iterations": float(sum(r["iterations"] for r in sres) / len(sres)),
+               "mean_coarse_iterations": float(sum(r["coarse_iterations"] for r in sres) / len(sres)),
+               "mean_final_residual_ratio": float(np.mean([r["residual"] / r["res0"] for r in sres if r["res0"] > 0])),
+               "max_abs_dCL_vs_unsequenced": max((abs(a["CL"] - b["CL"]) for a, b in cold), default=None)}
     plain, _ = serve.plain_loop(reqs, args.serve_rate / ws, seed=7 + rank)
     plat = serve.latency_stats([dict(r, t_done=r["t_done"], t_submit=r["t_submit"]) for r in plain])
     pspan = max(r["t_done"] for r in plain) - min(r["t_submit"] for r in plain)
@@ -256,7 +271,8 @@ def bench_served(aero, args, ws, rank, local):
             "plain_p99_s": plat["p99_s"], "speedup_vs_plain": pspan / span,
             "warm_starts": st["warm_starts"], "rounds": st["rounds"],
             "mean_iterations": float(sum(r["iterations"] for r in res) / len(res)),
-            "max_abs_dCL_cold_vs_plain": dcl}
+            "mean_final_residual_ratio": float(np.mean([r["residual"] / r["res0"] for r in res if r["res0"] > 0])),
+            "max_abs_dCL_cold_vs_plain": dcl, "sequenced": seq}
 
 
 def run_reference(args, ws, rank):

@@ -164,6 +164,16 @@ int a3d_solver_mach_max(a3d_solver* s, int32_t stride, double* mmax);
  * states (rho, u, v, w, p) at n points xyz (FP64, x/y/z interleaved), so that surfaces,
  * slices and probes need no full read().  ok[p] = 0 where no fluid cell is near.        */
 int a3d_solver_sample(a3d_solver* s, int32_t n, const double* xyz, double* out5, int32_t* ok);
+/* Grid sequencing, interpState (src/app_cfd.js:322-357, called from setupCFD :271-278):
+ * overwrite `fine`'s state with `coarse`'s current state interpolated onto its cells - a
+ * coarse pre-converged start for a finer grid of the same geometry.  Trilinear over the eight
+ * surrounding coarse centres with non-fluid corners dropped and the weights renormalised; the
+ * nearest fluid coarse cell within +-3 cells if all eight are excluded; else the free stream.
+ * Non-fluid target cells take the free stream (as after reset).  Resets `fine`'s iteration
+ * count and residual snapshot like a3d_solver_reset.  Both solvers on one device; the copy
+ * is ordered after the work already queued on `coarse` and before any work queued on it later.
+ * The reference's function is 2-D (axisymmetric v2 solver); this is its 3-D form.        */
+int a3d_solver_interp_state(a3d_solver* fine, const a3d_solver* coarse);
 /* Stage kernel selection; no counterpart in the reference (it has one shader).
  * kernel 0: one thread per cell evaluating its six faces (the reference's structure);
  * kernel 1: z-marching tiles that evaluate every face once, plain loads;
@@ -216,6 +226,15 @@ typedef struct a3d_server_config {
   int32_t device;
   int32_t warm_start;          /* 1: keep finished cases resident for reuse              */
   int32_t kz;                  /* batch tile depth (z planes); 0: default               */
+  /* Grid sequencing (the reference's setupCFD, src/app_cfd.js:271-278, 398-403): a cold
+   * request first solves a coarse case of cells/sequence cells until its residual dropped by
+   * sequence_drop or it ran sequence_max_iters iterations, then starts the requested case
+   * from that state (a3d_solver_interp_state).  0 or 1: off.  The requested case's res0 is
+   * its own first residual from the free stream, measured over one chunk before the
+   * interpolation, so residual_drop means the same with and without sequencing.           */
+  int32_t sequence;
+  int32_t sequence_max_iters;
+  double sequence_drop;
 } a3d_server_config;
 
 typedef struct a3d_request {
@@ -235,6 +254,7 @@ typedef struct a3d_result {
   double CL, CD, Cm, CDi;
   double residual, res0;       /* last and first density residual                       */
   double t_submit, t_admit, t_done;  /* seconds on the server's clock                   */
+  int64_t coarse_iterations;   /* iterations of the sequencing coarse case (0 if none)     */
 } a3d_result;
 
 typedef struct a3d_server a3d_server;

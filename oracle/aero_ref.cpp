@@ -749,3 +749,69 @@ int sample_one(const RefSolver<ST>& s, double x, double y, double z, double* out
 extern "C" void ref_solver_sample(void* h, int n, const double* xyz, double* out5, int* ok) {
   DISPATCH(h, for (int p = 0; p < n; p++) ok[p] = sample_one(*S_, xyz[3 * p], xyz[3 * p + 1], xyz[3 * p + 2], out5 + 5 * p));
 }
+
+/* ---- grid sequencing: interpState (src/app_cfd.js:322-357), restated in 3-D ----
+ * The reference interpolates a converged coarse state onto the target grid before solving
+ * there (setupCFD, src/app_cfd.js:271-278): bilinear weights over the four surrounding coarse
+ * centres, solid corners skipped and the weights renormalised; the nearest fluid cell within
+ * +-3 cells when every corner is solid; the free stream when none is found.  Here: trilinear
+ * over eight corners (x fastest, then y, then z; weight (wx*wy)*wz), "fluid" = type 0, and
+ * target cells that are not fluid take the free stream, as reset() gives them. */
+namespace {
+double frac_idx(const std::vector<float>& a, double v) {  // fracIdx, src/app_cfd.js:322-327
+  const int n = (int)a.size();
+  if (v <= a[0]) return (v - a[0]) / ((double)a[1] - a[0]);
+  if (v >= a[n - 1]) return n - 1 + (v - a[n - 1]) / ((double)a[n - 1] - a[n - 2]);
+  int lo = 0, hi = n - 1;
+  while (hi - lo > 1) { const int m = (lo + hi) >> 1; if (a[m] <= v) lo = m; else hi = m; }
+  return lo + (v - a[lo]) / ((double)a[hi] - a[lo]);
+}
+void axis_map(const std::vector<float>& cA, const std::vector<float>& cB, std::vector<int>& i0, std::vector<double>& t) {
+  const int n = (int)cA.size();
+  i0.resize(cB.size()); t.resize(cB.size());
+  for (size_t b = 0; b < cB.size(); b++) {
+    const double f = frac_idx(cA, cB[b]);
+    const int i = std::min(std::max((int)std::floor(f), 0), n - 1);
+    i0[b] = i; t[b] = std::min(std::max(f - i, 0.0), 1.0);
+  }
+}
+template <typename ST>
+void interp_state(RefSolver<ST>& B, const RefSolver<ST>& A) {
+  const Grid &gA = A.G, &gB = B.G;
+  std::vector<int> ix, iy, iz; std::vector<double> tx, ty, tz;
+  axis_map(gA.Xc, gB.Xc, ix, tx); axis_map(gA.Yc, gB.Yc, iy, ty); axis_map(gA.Zc, gB.Zc, iz, tz);
+  const long NXA = gA.NX, NYA = gA.NY;
+  for (int k = 0; k < gB.NZ; k++) for (int j = 0; j < gB.NY; j++) for (int i = 0; i < gB.NX; i++) {
+    const long qB = ((long)k * gB.NY + j) * gB.NX + i;
+    if (B.t[qB] != 0) { for (int c = 0; c < 5; c++) B.Q[c][qB] = (ST)B.F[c]; continue; }
+    double acc[5] = {0, 0, 0, 0, 0}, wsum = 0;
+    for (int dk = 0; dk < 2; dk++) for (int dj = 0; dj < 2; dj++) for (int di = 0; di < 2; di++) {
+      const double w = ((di ? tx[i] : 1 - tx[i]) * (dj ? ty[j] : 1 - ty[j])) * (dk ? tz[k] : 1 - tz[k]);
+      const long a = std::min(ix[i] + di, gA.NX - 1), b = std::min(iy[j] + dj, gA.NY - 1), c = std::min(iz[k] + dk, gA.NZ - 1);
+      const long qA = (c * NYA + b) * NXA + a;
+      if (A.t[qA] != 0 || w <= 0) continue;
+      for (int v = 0; v < 5; v++) acc[v] += w * (double)A.Q[v][qA];
+      wsum += w;
+    }
+    if (wsum > 0) { for (int v = 0; v < 5; v++) B.Q[v][qB] = (ST)(acc[v] / wsum); continue; }
+    long best = -1; int bd = 1 << 30;
+    for (int dk = -3; dk <= 3; dk++) for (int dj = -3; dj <= 3; dj++) for (int di = -3; di <= 3; di++) {
+      const long a = std::min(std::max(ix[i] + di, 0), gA.NX - 1), b = std::min(std::max(iy[j] + dj, 0), gA.NY - 1),
+                 c = std::min(std::max(iz[k] + dk, 0), gA.NZ - 1);
+      const long qA = (c * NYA + b) * NXA + a;
+      const int d2 = di * di + dj * dj + dk * dk;
+      if (A.t[qA] == 0 && d2 < bd) { bd = d2; best = qA; }
+    }
+    for (int v = 0; v < 5; v++) B.Q[v][qB] = best < 0 ? (ST)B.F[v] : A.Q[v][best];
+  }
+  B.it = 0; B.havePrev = false; B.prevIt = 0;
+}
+}  // namespace
+
+// Interpolates coarse solver `a` onto target solver `b`; both float32 (prec 32) or both float64.
+extern "C" int ref_interp_state(void* b, void* a) {
+  AnySolver *B = (AnySolver*)b, *A = (AnySolver*)a;
+  if (A->prec != B->prec) return 1;
+  if (A->prec == 64) interp_state(*B->s64, *A->s64); else interp_state(*B->s32, *A->s32);
+  return 0;
+}

@@ -206,3 +206,12 @@ def sample(solver, xyz):
     ok = np.zeros(len(xyz), np.int32)
     lb.ref_solver_sample(solver._h, len(xyz), xyz.reshape(-1), out.reshape(-1), ok)
     return out, ok.astype(bool)
+
+
+def interp_state(coarse, fine):
+    """Grid sequencing (interpState, src/app_cfd.js:322-357, restated in 3-D): fine's state from coarse's."""
+    lb = lib()
+    lb.ref_interp_state.argtypes = [C.c_void_p, C.c_void_p]
+    lb.ref_interp_state.restype = C.c_int
+    assert lb.ref_interp_state(fine._h, coarse._h) == 0
+    return fine

@@ -48,3 +48,22 @@ def test_request_beyond_the_budget_is_refused(aero):
         sv.submit(dict(REQS[0], cells=2.0e7))
     assert e.value.status == 6
     sv.close()
+
+
+def test_grid_sequencing_matches_cold_solves(aero):
+    """Sequenced requests (coarse case at cells/8 first, then interpState onto the requested grid)
+    converge to the cold solution in fewer iterations on the requested grid, with the same res0."""
+    serve = importlib.import_module("3d_aero_lab_b200.serve")
+    kw = dict(max_active=8, chunk=50, max_iters=3000, residual_drop=1e-2, warm_start=False)
+    runs = {}
+    for seq in (0, 8):
+        sv = serve.Server(sequence=seq, sequence_drop=0.05, sequence_max_iters=1500, **kw)
+        runs[seq] = [sv.wait(sv.submit(r), 600) for r in REQS]
+        sv.close()
+    for cold, seq in zip(runs[0], runs[8]):
+        assert cold["status"] == 0 and seq["status"] == 0
+        assert cold["coarse_iterations"] == 0 and seq["coarse_iterations"] > 0
+        assert seq["res0"] == cold["res0"]  # the requested case's own free-stream res0, bit for bit
+        for k in ("CL", "CD"):
+            assert abs(seq[k] - cold[k]) < 1e-3, (k, seq[k], cold[k])
+    assert sum(s["iterations"] for s in runs[8]) < sum(c["iterations"] for c in runs[0])
