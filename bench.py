@@ -256,7 +256,7 @@ def bench_served(aero, args, ws, rank, local):
         seq = {"sequence": args.serve_sequence, "solves_per_s": args.serve_requests / sspan, "p50_s": slat["p50_s"],
                "p99_s": slat["p99_s"], "mean_iterations": float(sum(r["iterations"] for r in sres) / len(sres)),
                "mean_coarse_iterations": float(sum(r["coarse_iterations"] for r in sres) / len(sres)),
-               "mean_final_residual_ratio": float(np.mean([r["residual"] / r["res0"] for r in sres if r["res0"] > 0])),
+               "mean_final_residual_ratio": statistics.fmean([r["residual"] / r["res0"] for r in sres if r["res0"] > 0]),
                "max_abs_dCL_vs_unsequenced": max((abs(a["CL"] - b["CL"]) for a, b in cold), default=None)}
     plain, _ = serve.plain_loop(reqs, args.serve_rate / ws, seed=7 + rank)
     plat = serve.latency_stats([dict(r, t_done=r["t_done"], t_submit=r["t_submit"]) for r in plain])
@@ -271,7 +271,7 @@ def bench_served(aero, args, ws, rank, local):
             "plain_p99_s": plat["p99_s"], "speedup_vs_plain": pspan / span,
             "warm_starts": st["warm_starts"], "rounds": st["rounds"],
             "mean_iterations": float(sum(r["iterations"] for r in res) / len(res)),
-            "mean_final_residual_ratio": float(np.mean([r["residual"] / r["res0"] for r in res if r["res0"] > 0])),
+            "mean_final_residual_ratio": statistics.fmean([r["residual"] / r["res0"] for r in res if r["res0"] > 0]),
             "max_abs_dCL_cold_vs_plain": dcl, "sequenced": seq}
 
 
