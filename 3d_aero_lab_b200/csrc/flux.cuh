@@ -25,8 +25,10 @@ __device__ __forceinline__ void cons_to_prim(float a0, float a1, float a2, float
   o[4] = fmaxf(kGm * (a4 - 0.5f * r * (u * u + v * v + w * w)), 1e-7f);
 }
 
-__device__ __forceinline__ float minmod(float a, float b) {  // mmod, src/air_cfd.js:196
-  return (a * b <= 0.f) ? 0.f : (fabsf(a) < fabsf(b) ? a : b);
+// mmod (src/air_cfd.js:196): 0 when a and b differ in sign, else the one nearer zero - the
+// median of (a, b, 0).  Four min/max instructions and no predicate.
+__device__ __forceinline__ float minmod(float a, float b) {
+  return fmaxf(fminf(a, b), fminf(fmaxf(a, b), 0.f));
 }
 
 // Rotate (rho, u, v, w, p) so that component d of the velocity becomes `un`.
@@ -41,8 +43,14 @@ __device__ __forceinline__ Prim rot(const float P[5], int d) {
 
 // HLLC flux with Davis wave-speed estimates (cfdHLLC, src/air_cfd.js:179-195).
 // Output: mass, normal momentum, tangential momenta, energy.
+// The star-region flux is the reference's, rearranged to need two divisions instead of four:
+// with d = S - u_K, q = rho_K d (both already formed for S_M) and g = 1/(S - S_M),
+//   rho* = q g,   F_t = v_t F_mass   (m v + S (rho* v - rho v) = v (m + S (rho* - rho))),
+//   E*   = rho* (E/rho + (S_M - u)(S_M + p/q)) = g (d E + (S_M - u)(q S_M + p)).
+// Sound speeds as g p rsqrt(g p rho).  Same values up to float32 rounding.
 __device__ __forceinline__ void hllc(const Prim& L, const Prim& R, float F[5]) {
-  const float aL = sqrtf(__fdividef(kG * L.p, L.r)), aR = sqrtf(__fdividef(kG * R.p, R.r));
+  const float gL = kG * L.p, gR = kG * R.p;
+  const float aL = gL * rsqrtf(gL * L.r), aR = gR * rsqrtf(gR * R.r);
   const float EL = L.p * (1.0f / kGm) + 0.5f * L.r * (L.un * L.un + L.u1 * L.u1 + L.u2 * L.u2);
   const float ER = R.p * (1.0f / kGm) + 0.5f * R.r * (R.un * R.un + R.u1 * R.u1 + R.u2 * R.u2);
   const float SL = fminf(L.un - aL, R.un - aR), SR = fmaxf(L.un + aL, R.un + aR);
@@ -53,19 +61,20 @@ __device__ __forceinline__ void hllc(const Prim& L, const Prim& R, float F[5]) {
     F[0] = m; F[1] = m * K.un + K.p; F[2] = m * K.u1; F[3] = m * K.u2; F[4] = K.un * (E + K.p);
     return;
   }
-  const float SM = __fdividef(R.p - L.p + L.r * L.un * (SL - L.un) - R.r * R.un * (SR - R.un),
-                              L.r * (SL - L.un) - R.r * (SR - R.un));
+  const float dL = SL - L.un, dR = SR - R.un;
+  const float qL = L.r * dL, qR = R.r * dR;
+  const float SM = __fdividef(R.p - L.p + qL * L.un - qR * R.un, qL - qR);
   const bool left = SM >= 0.f;
   const float rK = left ? L.r : R.r, uK = left ? L.un : R.un, v1 = left ? L.u1 : R.u1, v2 = left ? L.u2 : R.u2;
   const float pK = left ? L.p : R.p, EK = left ? EL : ER, S = left ? SL : SR;
-  const float f = __fdividef(rK * (S - uK), S - SM);
+  const float d = left ? dL : dR, q = left ? qL : qR;
+  const float g = __fdividef(1.0f, S - SM);
   const float m = rK * uK;
-  F[0] = m + S * (f - rK);
-  F[1] = m * uK + pK + S * (f * SM - m);
-  F[2] = m * v1 + S * (f * v1 - rK * v1);
-  F[3] = m * v2 + S * (f * v2 - rK * v2);
-  const float Es = f * (__fdividef(EK, rK) + (SM - uK) * (SM + __fdividef(pK, rK * (S - uK))));
-  F[4] = uK * (EK + pK) + S * (Es - EK);
+  F[0] = m + S * (q * g - rK);
+  F[1] = m * uK + pK + S * (q * g * SM - m);
+  F[2] = v1 * F[0];
+  F[3] = v2 * F[0];
+  F[4] = uK * (EK + pK) + S * (g * (d * EK + (SM - uK) * (q * SM + pK)) - EK);
 }
 
 // Flux through the face between cells b (left) and c (right) along one direction, with the
