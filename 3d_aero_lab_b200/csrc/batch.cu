@@ -31,23 +31,31 @@ struct __align__(128) BatchCase {
   long long tile_begin;
 };
 
+// Error record of a batch launch: [0] set once a tile's bounded wait ran out, [1] its table row,
+// [2] its tile number, [3] how many tiles the CTA had finished before it.
+constexpr int kErrWords = 4;
+
 template <bool STAGE2>
 __global__ void __launch_bounds__(TX * TY, 2)
     k_batch_stage(const BatchCase* __restrict__ cases, int ncases, long long total, int parity,
-                  unsigned long long* counter) {
+                  unsigned long long* counter, long long* err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   FusedSmem& S = *reinterpret_cast<FusedSmem*>(smem_raw);
-  __shared__ long long s_w;
+  __shared__ long long s_w, s_done;  // ticket; tiles this CTA finished (kept out of registers)
+  __shared__ int s_failed;
+  if (threadIdx.x == 0) { s_done = 0; s_failed = 0; }
   for (;;) {
     if (threadIdx.x == 0) s_w = (long long)atomicAdd(counter, 1ULL);
     __syncthreads();
     const long long w = s_w;
     __syncthreads();
     if (w >= total) {
-      // every CTA takes exactly one ticket past the end; the last one resets the queue
+      // every CTA takes exactly one ticket past the end (a CTA whose tile failed keeps taking
+      // tickets without work), so the last one can reset the queue for the next launch
       if (threadIdx.x == 0 && w == total + (long long)gridDim.x - 1) *counter = 0ULL;
       return;
     }
+    if (s_failed) continue;
     int lo = 0, hi = ncases - 1;
     while (lo < hi) {
       const int mid = (lo + hi + 1) >> 1;
@@ -60,7 +68,18 @@ __global__ void __launch_bounds__(TX * TY, 2)
     // stage 1: S1 = Q + dt R(Q); stage 2: B = Q/2 + (S1 + dt R(S1))/2
     const int qin = STAGE2 ? C.iS1 : iq;
     float* out = STAGE2 ? C.buf[ib] : C.buf[C.iS1];
-    if (!stage_tile<STAGE2>(S, &C.tmQ[qin], &C.tmC, C.a, C.buf[iq], out, bx, by, bz, C.kz)) return;
+    if (!stage_tile<STAGE2>(S, &C.tmQ[qin], &C.tmC, C.a, C.buf[iq], out, bx, by, bz, C.kz)) {
+      if (threadIdx.x == 0) {
+        s_failed = 1;
+        if (atomicCAS((unsigned long long*)err, 0ULL, 1ULL) == 0ULL) {
+          err[1] = lo;
+          err[2] = w;
+          err[3] = s_done;
+        }
+      }
+      continue;
+    }
+    if (threadIdx.x == 0) s_done++;
   }
 }
 
@@ -79,6 +98,7 @@ struct a3d_batch {
   std::vector<a3d::BatchCase> h_cases;
   std::vector<int> order;          // solver index of each table row (largest first)
   unsigned long long* d_counters = nullptr;
+  long long* d_err = nullptr;      // error record of the stage launches (kErrWords words)
   long long total = 0;
   int kz = 32;
   int ctas_per_sm = 2;
@@ -123,8 +143,10 @@ int build_table(a3d_batch* b) {
 int launch_pair(a3d_batch* b, int parity, cudaStream_t st) {
   const int grid = b->n_sm * b->ctas_per_sm, n = (int)b->solvers.size();
   const size_t smem = fused_smem_bytes();
-  k_batch_stage<false><<<grid, TX * TY, smem, st>>>(b->d_cases, n, b->total, parity, b->d_counters + 2 * parity);
-  k_batch_stage<true><<<grid, TX * TY, smem, st>>>(b->d_cases, n, b->total, parity, b->d_counters + 2 * parity + 1);
+  k_batch_stage<false><<<grid, TX * TY, smem, st>>>(b->d_cases, n, b->total, parity, b->d_counters + 2 * parity,
+                                                    b->d_err);
+  k_batch_stage<true><<<grid, TX * TY, smem, st>>>(b->d_cases, n, b->total, parity, b->d_counters + 2 * parity + 1,
+                                                   b->d_err);
   A3D_CUDA(cudaGetLastError());
   return A3D_OK;
 }
@@ -196,6 +218,8 @@ extern "C" int a3d_batch_create(a3d_solver* const* solvers, int32_t n, a3d_batch
   if (e == cudaSuccess) e = cudaMalloc(&b->d_cases, (size_t)n * sizeof(BatchCase));
   if (e == cudaSuccess) e = cudaMalloc(&b->d_counters, 8 * sizeof(unsigned long long));
   if (e == cudaSuccess) e = cudaMemsetAsync(b->d_counters, 0, 8 * sizeof(unsigned long long), b->st);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_err, kErrWords * sizeof(long long));
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->d_err, 0, kErrWords * sizeof(long long), b->st);
   if (e != cudaSuccess) { set_error("batch setup: %s", cudaGetErrorString(e)); rc = e == cudaErrorMemoryAllocation ? A3D_ERR_NOMEM : A3D_ERR_CUDA; }
   if (rc == A3D_OK) {
     int r = cudaFuncSetAttribute(k_batch_stage<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes());
@@ -214,6 +238,7 @@ extern "C" int a3d_batch_destroy(a3d_batch* b) {
   free_graph(b);
   cudaFree(b->d_cases);
   cudaFree(b->d_counters);
+  cudaFree(b->d_err);
   for (cudaEvent_t e : b->ev_in) if (e) cudaEventDestroy(e);
   if (b->ev_out) cudaEventDestroy(b->ev_out);
   if (b->st) cudaStreamDestroy(b->st);
@@ -253,6 +278,19 @@ extern "C" int a3d_batch_sync(a3d_batch* b) {
   A3D_ARG(b, "null batch");
   A3D_CUDA(cudaSetDevice(b->device));
   A3D_CUDA(cudaStreamSynchronize(b->st));
+  long long rec[kErrWords];
+  A3D_CUDA(cudaMemcpy(rec, b->d_err, sizeof(rec), cudaMemcpyDeviceToHost));
+  if (rec[0]) {
+    // clear the record (the queues were reset by the launches themselves) and report; the
+    // failed case keeps its own flag, so its solver reports the timeout until it is rebuilt
+    A3D_CUDA(cudaMemset(b->d_err, 0, sizeof(rec)));
+    const int row = (int)rec[1];
+    const a3d_solver* s = b->solvers[b->order[row]];
+    set_error("batch stage: a bounded wait ran out in case %d (%dx%dx%d cells), tile %lld, after %lld tiles on "
+              "that CTA", b->order[row], s->grid.NX, s->grid.NY, s->grid.NZ, rec[2] - b->h_cases[row].tile_begin,
+              rec[3]);
+    return A3D_ERR_TIMEOUT;
+  }
   for (a3d_solver* s : b->solvers) A3D_TRY(check_kernel_error(s));
   return A3D_OK;
 }

@@ -20,7 +20,7 @@ __device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b);
 __device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ float rcp(float a) { return __fdividef(1.0f, a); }
-__device__ __forceinline__ float sqrt(float a) { return sqrtf(a); }
+__device__ __forceinline__ float rsqrt(float a) { return rsqrtf(a); }
 __device__ __forceinline__ float min(float a, float b) { return fminf(a, b); }
 __device__ __forceinline__ float max(float a, float b) { return fmaxf(a, b); }
 __device__ __forceinline__ float splat(float s, float) { return s; }
@@ -31,7 +31,7 @@ __device__ __forceinline__ float2 sub(float2 a, float2 b) { return __fadd2_rn(a,
 __device__ __forceinline__ float2 mul(float2 a, float2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ float2 fma(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
 __device__ __forceinline__ float2 rcp(float2 a) { return make_float2(__fdividef(1.0f, a.x), __fdividef(1.0f, a.y)); }
-__device__ __forceinline__ float2 sqrt(float2 a) { return make_float2(sqrtf(a.x), sqrtf(a.y)); }
+__device__ __forceinline__ float2 rsqrt(float2 a) { return make_float2(rsqrtf(a.x), rsqrtf(a.y)); }
 __device__ __forceinline__ float2 min(float2 a, float2 b) { return make_float2(fminf(a.x, b.x), fminf(a.y, b.y)); }
 __device__ __forceinline__ float2 max(float2 a, float2 b) { return make_float2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }
 __device__ __forceinline__ float2 splat(float s, float2) { return make_float2(s, s); }
@@ -61,33 +61,34 @@ __device__ __forceinline__ PrimV<T> sel(M m, const PrimV<T>& a, const PrimV<T>& 
 
 // HLLC flux through faces with left/right states L, R (already reconstructed).
 // F = {mass, normal momentum, tangential momenta, energy}.
+// Star-region flux rearranged as in flux.cuh: d = S - u_K, q = rho_K d, g = 1/(S - S_M);
+// rho* = q g, tangential fluxes v_t F_mass, E* = g (d E + (S_M - u)(q S_M + p)); sound speeds
+// g p rsqrt(g p rho) - two reciprocals and two reciprocal square roots per face.
 template <class T>
 __device__ __forceinline__ void hllc(const PrimV<T>& L, const PrimV<T>& R, T F[5]) {
   const T g = splat(kG, L.r), igm = splat(1.0f / kGm, L.r), half = splat(0.5f, L.r);
-  const T irL = rcp(L.r), irR = rcp(R.r);
-  const T aL = sqrt(mul(mul(g, L.p), irL)), aR = sqrt(mul(mul(g, R.p), irR));
+  const T gL = mul(g, L.p), gR = mul(g, R.p);
+  const T aL = mul(gL, rsqrt(mul(gL, L.r))), aR = mul(gR, rsqrt(mul(gR, R.r)));
   const T kL = fma(L.un, L.un, fma(L.u1, L.u1, mul(L.u2, L.u2)));
   const T kR = fma(R.un, R.un, fma(R.u1, R.u1, mul(R.u2, R.u2)));
   const T EL = fma(L.p, igm, mul(mul(half, L.r), kL)), ER = fma(R.p, igm, mul(mul(half, R.r), kR));
   const T SL = min(sub(L.un, aL), sub(R.un, aR)), SR = max(add(L.un, aL), add(R.un, aR));
   const T mL = mul(L.r, L.un), mR = mul(R.r, R.un);
   const T dL = sub(SL, L.un), dR = sub(SR, R.un);
-  // contact speed SM = (pR - pL + mL dL - mR dR) / (rL dL - rR dR)
-  const T num = sub(fma(mL, dL, sub(R.p, L.p)), mul(mR, dR));
-  const T den = sub(mul(L.r, dL), mul(R.r, dR));
-  const T SM = mul(num, rcp(den));
+  const T qL = mul(L.r, dL), qR = mul(R.r, dR);
+  // contact speed SM = (pR - pL + qL uL - qR uR) / (qL - qR)
+  const T SM = mul(sub(fma(qL, L.un, sub(R.p, L.p)), mul(qR, R.un)), rcp(sub(qL, qR)));
   const auto left = ge0(SM);
   const PrimV<T> K = sel(left, L, R);
-  const T S = sel(left, SL, SR), EK = sel(left, EL, ER), irK = sel(left, irL, irR), mK = sel(left, mL, mR);
-  const T dK = sub(S, K.un);                       // S - uK
-  const T f = mul(mul(K.r, dK), rcp(sub(S, SM)));  // star density
-  const T fr = sub(f, K.r);
+  const T S = sel(left, SL, SR), EK = sel(left, EL, ER), mK = sel(left, mL, mR);
+  const T dK = sel(left, dL, dR), qK = sel(left, qL, qR);
+  const T gK = rcp(sub(S, SM));
   T Fs[5];
-  Fs[0] = fma(S, fr, mK);
-  Fs[1] = fma(S, fma(f, SM, neg(mK)), fma(mK, K.un, K.p));
-  Fs[2] = fma(mul(S, fr), K.u1, mul(mK, K.u1));
-  Fs[3] = fma(mul(S, fr), K.u2, mul(mK, K.u2));
-  const T Es = mul(f, fma(sub(SM, K.un), fma(mul(K.p, irK), rcp(dK), SM), mul(EK, irK)));
+  Fs[0] = fma(S, sub(mul(qK, gK), K.r), mK);
+  Fs[1] = fma(S, fma(mul(qK, gK), SM, neg(mK)), fma(mK, K.un, K.p));
+  Fs[2] = mul(K.u1, Fs[0]);
+  Fs[3] = mul(K.u2, Fs[0]);
+  const T Es = mul(gK, fma(sub(SM, K.un), fma(qK, SM, K.p), mul(dK, EK)));
   Fs[4] = fma(S, sub(Es, EK), mul(K.un, add(EK, K.p)));
   // supersonic fan: flux of the upwind state
   const auto supL = ge0(SL);
@@ -109,7 +110,7 @@ __device__ __forceinline__ void face_states(const float Pm[5], const float P[5],
 #pragma unroll
   for (int c = 0; c < 5; c++) {
     const float a = P[c] - Pm[c], b = Pp[c] - P[c];
-    const float s = ok ? (fmaxf(fminf(a, b), 0.f) + fminf(fmaxf(a, b), 0.f)) : 0.f;  // minmod
+    const float s = ok ? minmod(a, b) : 0.f;
     lo[c] = fmaf(-0.5f, s, P[c]);
     hi[c] = fmaf(0.5f, s, P[c]);
   }

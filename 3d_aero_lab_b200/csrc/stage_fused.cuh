@@ -105,8 +105,10 @@ __device__ __forceinline__ bool stage_tile(FusedSmem& S, const CUtensorMap* tmQp
     fence_barrier_init();
   }
   __syncthreads();
-  if (threadIdx.x == 0)
+  if (threadIdx.x == 0) {
+    fence_proxy_async_smem();  // earlier tiles' generic reads of the slots before these copies
     for (int p = k0 - 2; p <= k0 + 1; p++) issue_plane(S, &tmQ, &tmC, a, p, k0, i0, j0);
+  }
 
   // Column window: primitives of planes k, k+1 (W0, W1), the + z face state of plane k (Zh0)
   // and the flux of face k-1/2 (Gz, Az).
@@ -369,6 +371,11 @@ __device__ __forceinline__ bool stage_tile(FusedSmem& S, const CUtensorMap* tmQp
     drain(S, a, k0, first_pending, last_issued);
     return false;
   }
+  // every issued plane has been waited for: retire the ring barriers so that a persistent CTA
+  // can initialise them again for its next tile
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int s = 0; s < NSLOT; s++) mbar_inval(&S.bar[s]);
   return true;
 }
 
