@@ -43,15 +43,17 @@ __device__ __forceinline__ Prim sprim(const TmaSmem& S, int y, int x, int d) {
   return rot(P, d);
 }
 
+// x face between columns x-1 and x of shared-memory row y; `own`, when given, is the
+// primitive state of cell x already in registers (saves its five shared-memory loads).
 __device__ __forceinline__ float face_x(const StageArgs& a, const TmaSmem& S, int y, int x, int i, int j, int k,
-                                        float G[5]) {
+                                        float G[5], const float* own = nullptr) {
   const uint8_t cl = S.C[y][x - 1], cr = S.C[y][x];
   float A = 1.f;
   if (i - 1 >= 0 && (cl & C_IRR)) A = __ldg(a.ap0 + ((long)k * a.NY + j) * a.NX + (i - 1));
   if (A > 0.f) {
     float F[5];
-    face_flux(sprim(S, y, x - 2, 0), sprim(S, y, x - 1, 0), sprim(S, y, x, 0), sprim(S, y, x + 1, 0),
-              a.order2 && (cl & C_OKX), a.order2 && (cr & C_OKX), F);
+    face_flux(sprim(S, y, x - 2, 0), sprim(S, y, x - 1, 0), own ? rot(own, 0) : sprim(S, y, x, 0),
+              sprim(S, y, x + 1, 0), a.order2 && (cl & C_OKX), a.order2 && (cr & C_OKX), F);
     G[0] = A * F[0]; G[1] = A * F[1]; G[2] = A * F[2]; G[3] = A * F[3]; G[4] = A * F[4];
   } else {
     G[0] = G[1] = G[2] = G[3] = G[4] = 0.f;
@@ -60,14 +62,14 @@ __device__ __forceinline__ float face_x(const StageArgs& a, const TmaSmem& S, in
 }
 
 __device__ __forceinline__ float face_y(const StageArgs& a, const TmaSmem& S, int y, int x, int i, int j, int k,
-                                        float G[5]) {
+                                        float G[5], const float* own = nullptr) {
   const uint8_t cl = S.C[y - 1][x], cr = S.C[y][x];
   float A = 1.f;
   if (j - 1 >= 0 && (cl & C_IRR)) A = __ldg(a.ap1 + ((long)k * a.NY + (j - 1)) * a.NX + i);
   if (A > 0.f) {
     float F[5];
-    face_flux(sprim(S, y - 2, x, 1), sprim(S, y - 1, x, 1), sprim(S, y, x, 1), sprim(S, y + 1, x, 1),
-              a.order2 && (cl & C_OKY), a.order2 && (cr & C_OKY), F);
+    face_flux(sprim(S, y - 2, x, 1), sprim(S, y - 1, x, 1), own ? rot(own, 1) : sprim(S, y, x, 1),
+              sprim(S, y + 1, x, 1), a.order2 && (cl & C_OKY), a.order2 && (cr & C_OKY), F);
     G[0] = A * F[0]; G[1] = A * F[2]; G[2] = A * F[1]; G[3] = A * F[3]; G[4] = A * F[4];
   } else {
     G[0] = G[1] = G[2] = G[3] = G[4] = 0.f;
@@ -181,14 +183,14 @@ __global__ void __launch_bounds__(TX * TY, 3)
     // ---- face fluxes ----
     if (j < a.NY && i <= a.NX) {
       float G[5];
-      const float A = face_x(a, S, ty + 2, tx + 2, i, j, k, G);
+      const float A = face_x(a, S, ty + 2, tx + 2, i, j, k, G, W0);
 #pragma unroll
       for (int v = 0; v < 5; v++) S.Fx[v][ty][tx] = G[v];
       S.Ax[ty][tx] = A;
     }
     if (i < a.NX && j <= a.NY) {
       float G[5];
-      const float A = face_y(a, S, ty + 2, tx + 2, i, j, k, G);
+      const float A = face_y(a, S, ty + 2, tx + 2, i, j, k, G, W0);
 #pragma unroll
       for (int v = 0; v < 5; v++) S.Fy[v][ty][tx] = G[v];
       S.Ay[ty][tx] = A;
@@ -264,7 +266,7 @@ __global__ void __launch_bounds__(TX * TY, 3)
 #pragma unroll
           for (int c = 0; c < 5; c++) Pb[c] = W0[c];
         }
-        const float as = sqrtf(kG * Pb[4] / Pb[0]);
+        const float gp = kG * Pb[4], as = gp * rsqrtf(gp * Pb[0]);
         const float dt = a.cfl * fmaxf(ph, 0.25f) /
                          ((fabsf(Pb[1]) + as) * rx + (fabsf(Pb[2]) + as) * ry + (fabsf(Pb[3]) + as) * rz);
 #pragma unroll
