@@ -4,7 +4,9 @@
 // A device table holds, per case, its TMA maps, stage constants, state buffers and tile
 // counts; tiles of all cases are numbered consecutively (largest cases first).  The stage
 // kernel is persistent: a grid of (SM count x CTAs per SM) CTAs pulls tile numbers from a
-// global counter and runs the same fused tile as the single-case kernel (stage_fused.cuh).
+// global counter and runs the same tile as the single-case kernel: the TMA tile
+// (stage_tma.cuh, three CTAs per SM) for solvers on KERNEL_TMA, the packed fused tile
+// (stage_fused.cuh, two CTAs per SM) for solvers on KERNEL_FUSED.
 // The last CTA to find the queue empty resets the counter, so the four launches of two
 // SSP-RK2 iterations are captured once in a CUDA graph and replayed; buffer roles alternate
 // with the iteration's parity (Q and B swap every iteration, as in src/air_cfd.js:256).
@@ -14,12 +16,14 @@
 #include <numeric>
 #include <vector>
 #include "stage_fused.cuh"
+#include "stage_tma.cuh"
 
 namespace a3d {
 
 namespace {
 
-using namespace fused;
+using ring::TX;
+using ring::TY;
 
 struct __align__(128) BatchCase {
   CUtensorMap tmQ[3];  // maps over the case's three state buffers
@@ -35,12 +39,10 @@ struct __align__(128) BatchCase {
 // [2] its tile number, [3] how many tiles the CTA had finished before it.
 constexpr int kErrWords = 4;
 
-template <bool STAGE2>
-__global__ void __launch_bounds__(TX * TY, 2)
-    k_batch_stage(const BatchCase* __restrict__ cases, int ncases, long long total, int parity,
-                  unsigned long long* counter, long long* err) {
-  extern __shared__ __align__(128) unsigned char smem_raw[];
-  FusedSmem& S = *reinterpret_cast<FusedSmem*>(smem_raw);
+template <bool STAGE2, bool TMA_TILE>
+__device__ __forceinline__ void batch_loop(unsigned char* smem_raw, const BatchCase* __restrict__ cases, int ncases,
+                                           long long total, int parity, unsigned long long* counter,
+                                           long long* err) {
   __shared__ long long s_w, s_done;  // ticket; tiles this CTA finished (kept out of registers)
   __shared__ int s_failed;
   if (threadIdx.x == 0) { s_done = 0; s_failed = 0; }
@@ -68,7 +70,11 @@ __global__ void __launch_bounds__(TX * TY, 2)
     // stage 1: S1 = Q + dt R(Q); stage 2: B = Q/2 + (S1 + dt R(S1))/2
     const int qin = STAGE2 ? C.iS1 : iq;
     float* out = STAGE2 ? C.buf[ib] : C.buf[C.iS1];
-    if (!stage_tile<STAGE2>(S, &C.tmQ[qin], &C.tmC, C.a, C.buf[iq], out, bx, by, bz, C.kz)) {
+    const bool ok = TMA_TILE ? tma::stage_tile<STAGE2, true>(*reinterpret_cast<tma::TmaSmem*>(smem_raw), &C.tmQ[qin], &C.tmC,
+                                                       C.a, C.buf[iq], out, bx, by, bz, C.kz)
+                             : fused::stage_tile<STAGE2>(*reinterpret_cast<fused::FusedSmem*>(smem_raw), &C.tmQ[qin],
+                                                         &C.tmC, C.a, C.buf[iq], out, bx, by, bz, C.kz);
+    if (!ok) {
       if (threadIdx.x == 0) {
         s_failed = 1;
         if (atomicCAS((unsigned long long*)err, 0ULL, 1ULL) == 0ULL) {
@@ -81,6 +87,22 @@ __global__ void __launch_bounds__(TX * TY, 2)
     }
     if (threadIdx.x == 0) s_done++;
   }
+}
+
+template <bool STAGE2>
+__global__ void __launch_bounds__(TX * TY, 3)
+    k_batch_tma(const BatchCase* __restrict__ cases, int ncases, long long total, int parity,
+                unsigned long long* counter, long long* err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  batch_loop<STAGE2, true>(smem_raw, cases, ncases, total, parity, counter, err);
+}
+
+template <bool STAGE2>
+__global__ void __launch_bounds__(TX * TY, 2)
+    k_batch_fused(const BatchCase* __restrict__ cases, int ncases, long long total, int parity,
+                  unsigned long long* counter, long long* err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  batch_loop<STAGE2, false>(smem_raw, cases, ncases, total, parity, counter, err);
 }
 
 }  // namespace
@@ -102,6 +124,7 @@ struct a3d_batch {
   long long total = 0;
   int kz = 32;
   int ctas_per_sm = 2;
+  bool tma_tile = true;            // TMA tile (KERNEL_TMA solvers) or packed fused tile
   cudaGraphExec_t graph = nullptr;
   bool table_dirty = true;
 };
@@ -142,11 +165,16 @@ int build_table(a3d_batch* b) {
 
 int launch_pair(a3d_batch* b, int parity, cudaStream_t st) {
   const int grid = b->n_sm * b->ctas_per_sm, n = (int)b->solvers.size();
-  const size_t smem = fused_smem_bytes();
-  k_batch_stage<false><<<grid, TX * TY, smem, st>>>(b->d_cases, n, b->total, parity, b->d_counters + 2 * parity,
-                                                    b->d_err);
-  k_batch_stage<true><<<grid, TX * TY, smem, st>>>(b->d_cases, n, b->total, parity, b->d_counters + 2 * parity + 1,
-                                                   b->d_err);
+  unsigned long long* c0 = b->d_counters + 2 * parity;
+  if (b->tma_tile) {
+    const size_t smem = tma_smem_bytes();
+    k_batch_tma<false><<<grid, TX * TY, smem, st>>>(b->d_cases, n, b->total, parity, c0, b->d_err);
+    k_batch_tma<true><<<grid, TX * TY, smem, st>>>(b->d_cases, n, b->total, parity, c0 + 1, b->d_err);
+  } else {
+    const size_t smem = fused_smem_bytes();
+    k_batch_fused<false><<<grid, TX * TY, smem, st>>>(b->d_cases, n, b->total, parity, c0, b->d_err);
+    k_batch_fused<true><<<grid, TX * TY, smem, st>>>(b->d_cases, n, b->total, parity, c0 + 1, b->d_err);
+  }
   A3D_CUDA(cudaGetLastError());
   return A3D_OK;
 }
@@ -201,10 +229,13 @@ extern "C" int a3d_batch_create(a3d_solver* const* solvers, int32_t n, a3d_batch
     A3D_ARG(solvers[k], "null solver");
     A3D_ARG(solvers[k]->device == dev, "all solvers of a batch must live on one device");
     A3D_ARG(solvers[k]->kernel == KERNEL_FUSED || solvers[k]->kernel == KERNEL_TMA, "batch needs TMA-capable solvers");
+    A3D_ARG(solvers[k]->kernel == solvers[0]->kernel, "all solvers of a batch must select the same stage kernel");
   }
   A3D_CUDA(cudaSetDevice(dev));
   a3d_batch* b = new a3d_batch();
   b->device = dev;
+  b->tma_tile = solvers[0]->kernel == KERNEL_TMA;
+  b->ctas_per_sm = b->tma_tile ? 3 : 2;
   cudaDeviceGetAttribute(&b->n_sm, cudaDevAttrMultiProcessorCount, dev);
   b->solvers.assign(solvers, solvers + n);
   b->order.resize(n);
@@ -222,8 +253,13 @@ extern "C" int a3d_batch_create(a3d_solver* const* solvers, int32_t n, a3d_batch
   if (e == cudaSuccess) e = cudaMemsetAsync(b->d_err, 0, kErrWords * sizeof(long long), b->st);
   if (e != cudaSuccess) { set_error("batch setup: %s", cudaGetErrorString(e)); rc = e == cudaErrorMemoryAllocation ? A3D_ERR_NOMEM : A3D_ERR_CUDA; }
   if (rc == A3D_OK) {
-    int r = cudaFuncSetAttribute(k_batch_stage<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes());
-    if (r == cudaSuccess) r = cudaFuncSetAttribute(k_batch_stage<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fused_smem_bytes());
+    const int ft = (int)fused_smem_bytes(), tt = (int)tma_smem_bytes();
+    int r = cudaFuncSetAttribute(k_batch_fused<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ft);
+    if (r == cudaSuccess) r = cudaFuncSetAttribute(k_batch_fused<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ft);
+    if (r == cudaSuccess) r = cudaFuncSetAttribute(k_batch_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tt);
+    if (r == cudaSuccess) r = cudaFuncSetAttribute(k_batch_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tt);
+    if (r == cudaSuccess) r = cudaFuncSetAttribute(k_batch_tma<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (r == cudaSuccess) r = cudaFuncSetAttribute(k_batch_tma<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (r != cudaSuccess) { set_error("batch kernel attributes: %s", cudaGetErrorString((cudaError_t)r)); rc = A3D_ERR_CUDA; }
   }
   if (rc != A3D_OK) { a3d_batch_destroy(b); return rc; }
@@ -249,7 +285,7 @@ extern "C" int a3d_batch_destroy(a3d_batch* b) {
 extern "C" int a3d_batch_set_schedule(a3d_batch* b, int32_t kz, int32_t ctas_per_sm) {
   clear_error();
   A3D_ARG(b, "null batch");
-  A3D_ARG(kz >= 1 && kz <= 1024 && ctas_per_sm >= 1 && ctas_per_sm <= 2, "schedule");
+  A3D_ARG(kz >= 1 && kz <= 1024 && ctas_per_sm >= 1 && ctas_per_sm <= (b->tma_tile ? 3 : 2), "schedule");
   b->kz = kz;
   b->ctas_per_sm = ctas_per_sm;
   b->table_dirty = true;
@@ -319,7 +355,8 @@ extern "C" int a3d_batch_tune(a3d_batch* b, int32_t trial_iters, int32_t* best_k
   float best = 1e30f;
   int bkz = b->kz, bct = b->ctas_per_sm;
   const int kzs[] = {8, 16, 32, 64};
-  for (int ct = 1; ct <= 2 && rc == A3D_OK; ct++)
+  const int max_ct = b->tma_tile ? 3 : 2;
+  for (int ct = 1; ct <= max_ct && rc == A3D_OK; ct++)
     for (int kz : kzs) {
       if (rc != A3D_OK) break;
       a3d_batch_set_schedule(b, kz, ct);

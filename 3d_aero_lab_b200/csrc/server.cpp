@@ -138,12 +138,12 @@ void drop_coarse(a3d_server* sv, Job& j) {
 }
 
 // Coarse case done: the requested case measures its free-stream res0 over one chunk (on the
-// batch tile kernel, so the value is the one a cold batched run gets), then starts from the
+// batch's tile, so the value is the one a cold batched run gets), then starts from the
 // coarse state.  The probe chunk counts towards the case's iterations.
 int switch_to_target(a3d_server* sv, Job& j) {
   j.coarse_its = j.coarse->it;
   const int chunk = sv->cfg.chunk_iters;
-  int rc = a3d_solver_set_kernel(j.s, a3d::KERNEL_FUSED, sv->cfg.kz);
+  int rc = a3d_solver_set_kernel(j.s, a3d::KERNEL_TMA, sv->cfg.kz);
   if (rc == A3D_OK) rc = a3d_solver_step(j.s, chunk);
   double r0 = -1, dummy;
   if (rc == A3D_OK) rc = a3d_solver_residual(j.s, 1, &r0);
@@ -222,7 +222,10 @@ void finish_case(a3d_server* sv, Job& j, int status) {
 void scheduler(a3d_server* sv) {
   cudaSetDevice(sv->cfg.device);
   a3d_batch* batch = nullptr;
-  std::vector<a3d_solver*> batch_set;
+  // The batch is keyed by (request id, coarse phase), never by solver address: a finished
+  // case's solver is destroyed and the next one may be allocated at the same address, and a
+  // batch kept for it would still hold the old case's device table (buffers, tensor maps).
+  std::vector<std::pair<int64_t, int>> batch_key;
   for (;;) {
     std::vector<std::shared_ptr<Job>> admit;
     {
@@ -263,8 +266,12 @@ void scheduler(a3d_server* sv) {
     if (act.empty()) continue;
     // one round: all active cases advance together
     std::vector<a3d_solver*> set;
-    for (auto& j : act) set.push_back(j->coarse ? j->coarse : j->s);
-    if (set != batch_set) {
+    std::vector<std::pair<int64_t, int>> key;
+    for (auto& j : act) {
+      set.push_back(j->coarse ? j->coarse : j->s);
+      key.emplace_back(j->id, j->coarse ? 1 : 0);
+    }
+    if (!batch || key != batch_key) {
       if (batch) a3d_batch_destroy(batch);
       batch = nullptr;
       if (a3d_batch_create(set.data(), (int)set.size(), &batch) != A3D_OK) {
@@ -274,11 +281,13 @@ void scheduler(a3d_server* sv) {
         for (auto& j : act) finish_case(sv, *j, A3D_ERR_CUDA);
         sv->active.clear();
         sv->cv_done.notify_all();
-        batch_set.clear();
+        batch_key.clear();
         continue;
       }
-      a3d_batch_set_schedule(batch, sv->cfg.kz, 2);
-      batch_set = set;
+      int32_t kz0 = 0, ct0 = 0;  // keep the batch's default CTAs per SM for its tile
+      a3d_batch_get_schedule(batch, &kz0, &ct0, nullptr);
+      a3d_batch_set_schedule(batch, sv->cfg.kz, ct0);
+      batch_key = key;
     }
     int rc = a3d_batch_step(batch, sv->cfg.chunk_iters);
     if (rc == A3D_OK) rc = a3d_batch_sync(batch);

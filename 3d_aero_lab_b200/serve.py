@@ -141,9 +141,9 @@ def latency_stats(res):
             "mean_s": float(lat.mean()), "max_s": float(lat.max())}
 
 
-def solve_plain(r, residual_drop=1e-3, chunk=50, max_iters=3000, device=0, kernel=3):
-    """One request on its own solver, the same convergence rule as the server.  Kernel 3 is
-    the tile the server's batches run, so the two give bit-identical results."""
+def solve_plain(r, residual_drop=1e-3, chunk=50, max_iters=3000, device=0, kernel=2):
+    """One request on its own solver, the same convergence rule as the server.  Kernel 2 (TMA)
+    is the tile the server's batches run, so the two give bit-identical results."""
     ac, sh = aircraft(r["type"])
     g = cfd_grid(sh, r["cells"])
     s = CfdGPU(g, shape=sh, delta=r["delta"], device=device)

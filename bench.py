@@ -194,7 +194,7 @@ def bench_batched(aero, args, ws, rank, local):
     for r in reqs:
         c = aero.Case(aircraft_type=r["type"], cells=r["cells"], M=r["M"], alpha=r["alpha"], delta=r["delta"],
                       device=local)
-        c.solver.set_kernel(3, 16)  # the tile the batch runs: plain and batched results are bit-identical
+        c.solver.set_kernel(2, 16)  # the tile the batch runs (its tuned z run may round differently)
         cases.append(c)
     cells = sum(c.g.N for c in cases)
     it = args.batch_iters
