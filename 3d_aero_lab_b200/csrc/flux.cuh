@@ -83,21 +83,20 @@ __device__ __forceinline__ void hllc(const Prim& L, const Prim& R, float F[5]) {
 // order when a reconstructed density or pressure is not positive (src/air_cfd.js:221).
 __device__ __forceinline__ void face_flux(const Prim& a, const Prim& b, const Prim& c, const Prim& e, bool okL,
                                           bool okR, float F[5]) {
-  Prim L = b, R = c;
-  if (okL) {
-    L.r = b.r + 0.5f * minmod(b.r - a.r, c.r - b.r);
-    L.un = b.un + 0.5f * minmod(b.un - a.un, c.un - b.un);
-    L.u1 = b.u1 + 0.5f * minmod(b.u1 - a.u1, c.u1 - b.u1);
-    L.u2 = b.u2 + 0.5f * minmod(b.u2 - a.u2, c.u2 - b.u2);
-    L.p = b.p + 0.5f * minmod(b.p - a.p, c.p - b.p);
-  }
-  if (okR) {
-    R.r = c.r - 0.5f * minmod(c.r - b.r, e.r - c.r);
-    R.un = c.un - 0.5f * minmod(c.un - b.un, e.un - c.un);
-    R.u1 = c.u1 - 0.5f * minmod(c.u1 - b.u1, e.u1 - c.u1);
-    R.u2 = c.u2 - 0.5f * minmod(c.u2 - b.u2, e.u2 - c.u2);
-    R.p = c.p - 0.5f * minmod(c.p - b.p, e.p - c.p);
-  }
+  // Branch-free: the half-slope factor is 0 where the slope test failed, so the state is the
+  // cell value itself (b + 0 * s); the slopes of neighbouring finite states are finite.
+  const float hL = okL ? 0.5f : 0.f, hR = okR ? -0.5f : 0.f;
+  Prim L, R;
+  L.r = fmaf(hL, minmod(b.r - a.r, c.r - b.r), b.r);
+  L.un = fmaf(hL, minmod(b.un - a.un, c.un - b.un), b.un);
+  L.u1 = fmaf(hL, minmod(b.u1 - a.u1, c.u1 - b.u1), b.u1);
+  L.u2 = fmaf(hL, minmod(b.u2 - a.u2, c.u2 - b.u2), b.u2);
+  L.p = fmaf(hL, minmod(b.p - a.p, c.p - b.p), b.p);
+  R.r = fmaf(hR, minmod(c.r - b.r, e.r - c.r), c.r);
+  R.un = fmaf(hR, minmod(c.un - b.un, e.un - c.un), c.un);
+  R.u1 = fmaf(hR, minmod(c.u1 - b.u1, e.u1 - c.u1), c.u1);
+  R.u2 = fmaf(hR, minmod(c.u2 - b.u2, e.u2 - c.u2), c.u2);
+  R.p = fmaf(hR, minmod(c.p - b.p, e.p - c.p), c.p);
   if (L.r <= 0.f || L.p <= 0.f || R.r <= 0.f || R.p <= 0.f) { L = b; R = c; }
   hllc(L, R, F);
 }
