@@ -47,6 +47,9 @@ __device__ __forceinline__ Prim rot(const float P[5], int d) {
 // with d = S - u_K, q = rho_K d (both already formed for S_M) and g = 1/(S - S_M),
 //   rho* = q g,   F_t = v_t F_mass   (m v + S (rho* v - rho v) = v (m + S (rho* - rho))),
 //   E*   = rho* (E/rho + (S_M - u)(S_M + p/q)) = g (d E + (S_M - u)(q S_M + p)).
+// The supersonic cases need no branch: F = F_K + S' (U*_K - U_K) with S' = min(S_L, 0) on the
+// left of the contact and max(S_R, 0) on its right is the upwind state flux F_K exactly when
+// the fan is supersonic (S' = 0 makes every star term 0 * finite) and the star flux otherwise.
 // Sound speeds as g p rsqrt(g p rho).  Same values up to float32 rounding.
 __device__ __forceinline__ void hllc(const Prim& L, const Prim& R, float F[5]) {
   const float gL = kG * L.p, gR = kG * R.p;
@@ -54,21 +57,16 @@ __device__ __forceinline__ void hllc(const Prim& L, const Prim& R, float F[5]) {
   const float EL = L.p * (1.0f / kGm) + 0.5f * L.r * (L.un * L.un + L.u1 * L.u1 + L.u2 * L.u2);
   const float ER = R.p * (1.0f / kGm) + 0.5f * R.r * (R.un * R.un + R.u1 * R.u1 + R.u2 * R.u2);
   const float SL = fminf(L.un - aL, R.un - aR), SR = fmaxf(L.un + aL, R.un + aR);
-  if (SL >= 0.f || SR <= 0.f) {  // supersonic: upwind state flux
-    const bool left = SL >= 0.f;
-    const Prim& K = left ? L : R;
-    const float E = left ? EL : ER, m = K.r * K.un;
-    F[0] = m; F[1] = m * K.un + K.p; F[2] = m * K.u1; F[3] = m * K.u2; F[4] = K.un * (E + K.p);
-    return;
-  }
   const float dL = SL - L.un, dR = SR - R.un;
   const float qL = L.r * dL, qR = R.r * dR;
   const float SM = __fdividef(R.p - L.p + qL * L.un - qR * R.un, qL - qR);
   const bool left = SM >= 0.f;
   const float rK = left ? L.r : R.r, uK = left ? L.un : R.un, v1 = left ? L.u1 : R.u1, v2 = left ? L.u2 : R.u2;
-  const float pK = left ? L.p : R.p, EK = left ? EL : ER, S = left ? SL : SR;
+  const float pK = left ? L.p : R.p, EK = left ? EL : ER;
+  const float S = left ? fminf(SL, 0.f) : fmaxf(SR, 0.f);
   const float d = left ? dL : dR, q = left ? qL : qR;
-  const float g = __fdividef(1.0f, S - SM);
+  // where S' = 0 the star terms are multiplied away; keep their divisor finite there
+  const float g = __fdividef(1.0f, S != 0.f ? (left ? SL : SR) - SM : 1.f);
   const float m = rK * uK;
   F[0] = m + S * (q * g - rK);
   F[1] = m * uK + pK + S * (q * g * SM - m);
