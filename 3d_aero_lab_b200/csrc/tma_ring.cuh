@@ -29,23 +29,23 @@ struct __align__(128) Slot {
 // src/air_cfd.js:205-210 (far field outside x, z and +y; mirror with v negated below y = 0).
 __device__ __forceinline__ uint8_t slot_cell(const StageArgs& a, const Slot& s, int i, int j, int k, int i0, int j0,
                                              float P[5]) {
-  if (i < 0 || i >= a.NX || k < 0 || k >= a.NZ || j >= a.NY) {
-#pragma unroll
-    for (int v = 0; v < 5; v++) P[v] = a.Pff[v];
-    return T_GHOST;
-  }
+  // Converted without branches, then overridden by selects: for every cell a tile reads (its
+  // columns and the 2-cell halo) the slot indices below stay inside the slot, and whatever a
+  // ghost's slot position holds (another plane, or nothing loaded) is replaced.
+  const bool ghost = i < 0 || i >= a.NX || k < 0 || k >= a.NZ || j >= a.NY;
   const bool mirror = j < 0;
   const int y = (mirror ? -1 - j : j) - j0 + 2, xq = i - i0 + 4;
   const uint8_t c = s.C[y][i - i0 + 16];
   const int t = c & 7;
-  if (t >= T_SINK) {
+  cons_to_prim(s.Q[0][y][xq], s.Q[1][y][xq], s.Q[2][y][xq], s.Q[3][y][xq], s.Q[4][y][xq], P);
+  if (!ghost && t >= T_SINK) {  // fixed-state cell (rare)
 #pragma unroll
     for (int v = 0; v < 5; v++) P[v] = a.Pfix[t - T_SINK][v];
-  } else {
-    cons_to_prim(s.Q[0][y][xq], s.Q[1][y][xq], s.Q[2][y][xq], s.Q[3][y][xq], s.Q[4][y][xq], P);
   }
-  if (mirror) { P[2] = -P[2]; return T_MIRROR; }
-  return c;
+#pragma unroll
+  for (int v = 0; v < 5; v++) P[v] = ghost ? a.Pff[v] : P[v];
+  P[2] = (mirror && !ghost) ? -P[2] : P[2];
+  return ghost ? (uint8_t)T_GHOST : mirror ? (uint8_t)T_MIRROR : c;
 }
 
 // Slot of plane p for a CTA whose run starts at k0 (the ring starts with plane k0-2), and the
