@@ -75,6 +75,17 @@ __device__ __forceinline__ void hllc(const Prim& L, const Prim& R, float F[5]) {
   F[4] = uK * (EK + pK) + S * (g * (d * EK + (SM - uK) * (q * SM + pK)) - EK);
 }
 
+// Flux from reconstructed face states L, R of the cells b (left) and c (right): first order
+// (b, c) when a reconstructed density or pressure is not positive (src/air_cfd.js:221).
+__device__ __forceinline__ void face_flux_lr(Prim L, Prim R, const Prim& b, const Prim& c, float F[5]) {
+  const bool bad = L.r <= 0.f || L.p <= 0.f || R.r <= 0.f || R.p <= 0.f;  // selects, not a branch
+  L.r = bad ? b.r : L.r; L.un = bad ? b.un : L.un; L.u1 = bad ? b.u1 : L.u1; L.u2 = bad ? b.u2 : L.u2;
+  L.p = bad ? b.p : L.p;
+  R.r = bad ? c.r : R.r; R.un = bad ? c.un : R.un; R.u1 = bad ? c.u1 : R.u1; R.u2 = bad ? c.u2 : R.u2;
+  R.p = bad ? c.p : R.p;
+  hllc(L, R, F);
+}
+
 // Flux through the face between cells b (left) and c (right) along one direction, with the
 // neighbours a (left of b) and e (right of c).  okL/okR: the slope test at b and c passed
 // (three fluid cells and both faces fully open, src/air_cfd.js:213-216).  Falls back to first
@@ -95,8 +106,7 @@ __device__ __forceinline__ void face_flux(const Prim& a, const Prim& b, const Pr
   R.u1 = fmaf(hR, minmod(c.u1 - b.u1, e.u1 - c.u1), c.u1);
   R.u2 = fmaf(hR, minmod(c.u2 - b.u2, e.u2 - c.u2), c.u2);
   R.p = fmaf(hR, minmod(c.p - b.p, e.p - c.p), c.p);
-  if (L.r <= 0.f || L.p <= 0.f || R.r <= 0.f || R.p <= 0.f) { L = b; R = c; }
-  hllc(L, R, F);
+  face_flux_lr(L, R, b, c, F);
 }
 
 // Scatter a rotated-frame flux back to (mass, x-, y-, z-momentum, energy).

@@ -77,13 +77,25 @@ __device__ __forceinline__ float face_y(const StageArgs& a, const TmaSmem& S, in
   return A;
 }
 
-__device__ __forceinline__ float face_z(const StageArgs& a, const float Pa[5], const float Pb[5], const float Pc[5],
-                                        const float Pe[5], uint8_t cb, uint8_t cc, bool in_dom_b, long qb, float G[5]) {
+// z face between cell b (plane k) and cell c (plane k+1) of the column.  Lb is b's +z face
+// state, carried from the face below; c's slope gives this face's right state and, in Lc, the
+// left state of the face above: each z slope is formed once.  Same numbers as face_flux.
+__device__ __forceinline__ float face_z_carry(const StageArgs& a, const float Lb[5], const float Pb[5],
+                                              const float Pc[5], const float Pe[5], uint8_t cb, uint8_t cc,
+                                              bool in_dom_b, long qb, float G[5], float Lc[5]) {
+  const float h = (a.order2 && (cc & C_OKZ)) ? 0.5f : 0.f;
+  float Rc[5];
+#pragma unroll
+  for (int v = 0; v < 5; v++) {
+    const float sl = minmod(Pc[v] - Pb[v], Pe[v] - Pc[v]);
+    Rc[v] = fmaf(-h, sl, Pc[v]);
+    Lc[v] = fmaf(h, sl, Pc[v]);
+  }
   float A = 1.f;
   if (in_dom_b && (cb & C_IRR)) A = __ldg(a.ap2 + qb);
   if (A > 0.f) {
     float F[5];
-    face_flux(rot(Pa, 2), rot(Pb, 2), rot(Pc, 2), rot(Pe, 2), a.order2 && (cb & C_OKZ), a.order2 && (cc & C_OKZ), F);
+    face_flux_lr(rot(Lb, 2), rot(Rc, 2), rot(Pb, 2), rot(Pc, 2), F);
     G[0] = A * F[0]; G[1] = A * F[2]; G[2] = A * F[3]; G[3] = A * F[1]; G[4] = A * F[4];
   } else {
     G[0] = G[1] = G[2] = G[3] = G[4] = 0.f;
@@ -121,11 +133,11 @@ __device__ __forceinline__ bool stage_tile(TmaSmem& S, const CUtensorMap* tmQ, c
   }
 
   bool ok = true;
-  float Wm[5], W0[5], W1[5], W2[5];
+  float Lz[5], W0[5], W1[5], W2[5];  // Lz: +z face state of the plane-k cell (carried)
   uint8_t cm, c0, c1, c2;
   float Gz[5], Az = 1.f;
   {
-    float Wa[5];
+    float Wa[5], Wm[5], Lm[5];
     ok &= mbar_wait(&S.bar[slot_of(k0 - 2, k0)], parity_of(k0 - 2, k0));
     slot_cell(a, S.slot[slot_of(k0 - 2, k0)], i, j, k0 - 2, i0, j0, Wa);
     ok &= mbar_wait(&S.bar[slot_of(k0 - 1, k0)], parity_of(k0 - 1, k0));
@@ -136,7 +148,12 @@ __device__ __forceinline__ bool stage_tile(TmaSmem& S, const CUtensorMap* tmQ, c
     c1 = slot_cell(a, S.slot[slot_of(k0 + 1, k0)], i, j, k0 + 1, i0, j0, W1);
 #pragma unroll
     for (int c = 0; c < 5; c++) Gz[c] = 0.f;
-    if (in_dom) Az = face_z(a, Wa, Wm, W0, W1, cm, c0, k0 - 1 >= 0, ((long)(k0 - 1) * a.NY + j) * a.NX + i, Gz);
+    {
+      const float hm = (a.order2 && (cm & C_OKZ)) ? 0.5f : 0.f;
+#pragma unroll
+      for (int v = 0; v < 5; v++) Lm[v] = fmaf(hm, minmod(Wm[v] - Wa[v], W0[v] - Wm[v]), Wm[v]);
+    }
+    if (in_dom) Az = face_z_carry(a, Lm, Wm, W0, W1, cm, c0, k0 - 1 >= 0, ((long)(k0 - 1) * a.NY + j) * a.NX + i, Gz, Lz);
   }
   if (!ok) S.abort = 1;
   __syncthreads();  // slots of planes k0-2 and k0-1 are free again
@@ -220,7 +237,8 @@ __device__ __forceinline__ bool stage_tile(TmaSmem& S, const CUtensorMap* tmQ, c
       }
     }
     float Gn[5], An = 1.f;
-    if (in_dom) An = face_z(a, Wm, W0, W1, W2, c0, c1, true, q, Gn);
+    float Ln[5];
+    if (in_dom) An = face_z_carry(a, Lz, W0, W1, W2, c0, c1, true, q, Gn, Ln);
     __syncthreads();
     // ---- residual and RK update ----
     if (in_dom) {
@@ -287,7 +305,7 @@ __device__ __forceinline__ bool stage_tile(TmaSmem& S, const CUtensorMap* tmQ, c
       for (int c = 0; c < 5; c++) Outp[c * Np + qp] = o[c];
     }
 #pragma unroll
-    for (int c = 0; c < 5; c++) { Gz[c] = Gn[c]; Wm[c] = W0[c]; W0[c] = W1[c]; W1[c] = W2[c]; }
+    for (int c = 0; c < 5; c++) { Gz[c] = Gn[c]; Lz[c] = Ln[c]; W0[c] = W1[c]; W1[c] = W2[c]; }
     Az = An;
     cm = c0; c0 = c1; c1 = c2;
     (void)cm;
