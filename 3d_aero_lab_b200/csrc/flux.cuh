@@ -79,21 +79,26 @@ __device__ __forceinline__ void hllc(const Prim& L, const Prim& R, float F[5]) {
   F[4] = uK * (EK + pK) + S * (g * (d * EK + (SM - uK) * (q * SM + pK)) - EK);
 }
 
-// Flux from reconstructed face states L, R of the cells b (left) and c (right): first order
-// (b, c) when a reconstructed density or pressure is not positive (src/air_cfd.js:221).
-__device__ __forceinline__ void face_flux_lr(Prim L, Prim R, const Prim& b, const Prim& c, float F[5]) {
-  const bool bad = L.r <= 0.f || L.p <= 0.f || R.r <= 0.f || R.p <= 0.f;  // selects, not a branch
-  L.r = bad ? b.r : L.r; L.un = bad ? b.un : L.un; L.u1 = bad ? b.u1 : L.u1; L.u2 = bad ? b.u2 : L.u2;
-  L.p = bad ? b.p : L.p;
-  R.r = bad ? c.r : R.r; R.un = bad ? c.un : R.un; R.u1 = bad ? c.u1 : R.u1; R.u2 = bad ? c.u2 : R.u2;
-  R.p = bad ? c.p : R.p;
+// Flux from reconstructed face states L, R of the cells b (left) and c (right).
+//
+// The reference falls back to first order (L = b, R = c) when a reconstructed density or
+// pressure is not positive (src/air_cfd.js:221).  Here that can never happen, so the test is
+// left out and the fluxes are the same bit for bit:
+//   * every primitive state a face reads has density >= 1e-6 and pressure >= 1e-7: cell values
+//     through cons_to_prim's floors, far-field and fixed states through the same floors on the
+//     host (prim_of in solver.cu), mirror ghosts are cell values with v negated;
+//   * a minmod-limited state is b + s/2 with s = 0, or s of the sign of both differences and no
+//     larger than |c - b|; it therefore lies between b and (b + c) / 2 > 0, and its float32
+//     value, rounded from at least (b + c) / 2 - b * 2^-25, stays positive;
+//   * with NaN inputs the reference's comparisons are false as well.
+__device__ __forceinline__ void face_flux_lr(const Prim& L, const Prim& R, const Prim&, const Prim&, float F[5]) {
   hllc(L, R, F);
 }
 
 // Flux through the face between cells b (left) and c (right) along one direction, with the
 // neighbours a (left of b) and e (right of c).  okL/okR: the slope test at b and c passed
-// (three fluid cells and both faces fully open, src/air_cfd.js:213-216).  Falls back to first
-// order when a reconstructed density or pressure is not positive (src/air_cfd.js:221).
+// (three fluid cells and both faces fully open, src/air_cfd.js:213-216).  The reference's
+// first-order fallback (src/air_cfd.js:221) cannot fire here (face_flux_lr says why).
 __device__ __forceinline__ void face_flux(const Prim& a, const Prim& b, const Prim& c, const Prim& e, bool okL,
                                           bool okR, float F[5]) {
   // Branch-free: the half-slope factor is 0 where the slope test failed, so the state is the
