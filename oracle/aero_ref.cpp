@@ -17,6 +17,7 @@
  *
  * Only tests/, __graft_entry__.smoke() and bench.py's CPU baseline load this library.
  */
+#include <atomic>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -419,6 +420,10 @@ void cfdHLLC(const double* L, const double* R, int d, double* out) {  // src/air
 
 inline double mmod(double a, double b) { return a * b <= 0 ? 0 : std::fabs(a) < std::fabs(b) ? a : b; }  // src/air_cfd.js:196
 
+// How often the first-order fallback of src/air_cfd.js:221 has fired since the last reset
+// (the tests check that it never does for the states this scheme produces).
+std::atomic<long> g_fallbacks{0};
+
 template <typename ST>
 struct RefSolver {
   Grid G;
@@ -485,8 +490,10 @@ struct RefSolver {
         if (a <= 0) continue;
         const int lo = sg > 0 ? 0 : -1;
         for (int v = 0; v < 5; v++) { L[v] = P[5 * (lo + 2) + v] + 0.5 * s[5 * (lo + 1) + v]; Rr[v] = P[5 * (lo + 3) + v] - 0.5 * s[5 * (lo + 2) + v]; }
-        if (L[0] <= 0 || L[4] <= 0 || Rr[0] <= 0 || Rr[4] <= 0)
+        if (L[0] <= 0 || L[4] <= 0 || Rr[0] <= 0 || Rr[4] <= 0) {
           for (int v = 0; v < 5; v++) { L[v] = P[5 * (lo + 2) + v]; Rr[v] = P[5 * (lo + 3) + v]; }
+          g_fallbacks.fetch_add(1, std::memory_order_relaxed);  // counted for the tests
+        }
         cfdHLLC(L, Rr, d, fl);
         for (int c = 0; c < 5; c++) R[c] -= sg * a * fl[c] / h;
       }
@@ -814,4 +821,10 @@ extern "C" int ref_interp_state(void* b, void* a) {
   if (A->prec != B->prec) return 1;
   if (A->prec == 64) interp_state(*B->s64, *A->s64); else interp_state(*B->s32, *A->s32);
   return 0;
+}
+
+extern "C" long ref_fallback_count(int reset) {
+  const long n = g_fallbacks.load();
+  if (reset) g_fallbacks.store(0);
+  return n;
 }

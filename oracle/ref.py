@@ -215,3 +215,11 @@ def interp_state(coarse, fine):
     lb.ref_interp_state.restype = C.c_int
     assert lb.ref_interp_state(fine._h, coarse._h) == 0
     return fine
+
+
+def fallback_count(reset=False):
+    """How often the oracle's first-order fallback (src/air_cfd.js:221) has fired."""
+    lb = lib()
+    lb.ref_fallback_count.argtypes = [C.c_int]
+    lb.ref_fallback_count.restype = C.c_long
+    return int(lb.ref_fallback_count(1 if reset else 0))

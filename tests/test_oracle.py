@@ -94,3 +94,32 @@ def test_other_types_build_and_step(aero, ref, typ):
     if typ == "airliner":
         assert np.count_nonzero(geo.t == 3) > 0 and np.count_nonzero(geo.t == 4) > 0
     assert np.count_nonzero(geo.t == 5) > 0
+
+
+def test_first_order_fallback_never_fires(aero, ref):
+    """The reference falls back to first order when a reconstructed density or pressure is not
+    positive (src/air_cfd.js:221).  With the primitive floors (rho >= 1e-6, p >= 1e-7) a
+    minmod-limited state stays between its cell value and the midpoint to a neighbour, so the
+    fallback cannot fire; the device flux leaves it out on that ground.  Here the oracle, which
+    keeps it, counts it over the README case and over random cut-cell boxes with perturbed
+    states, fixed cells and baffles."""
+    import numpy as np
+    from helpers import BoxGrid, box_geometry, freestream, oracle_case
+    ref.fallback_count(reset=True)
+    *_, s = oracle_case(aero, ref, "fighter", 30000, 3.0, threads=8)
+    s.step(200)
+    for seed, dims in ((0, (9, 7, 6)), (1, (33, 9, 20)), (4, (24, 12, 18))):
+        rng = np.random.default_rng(seed)
+        bg = BoxGrid(rng, *dims)
+        geo = ref.Geom()
+        geo.t, geo.phi, geo.ap = box_geometry(rng, *dims)
+        o = ref.CfdCPU(bg, geo)
+        o.setFree(freestream(0.9, 4.0))
+        o.setFix([[1.1, 0.3, 0.0, 0.0, 2.1], [0.9, 0.8, 0.05, 0.0, 2.4], [0.7, 1.2, 0.0, -0.1, 3.0]])
+        o.reset()
+        Q = o.read()
+        Q = Q * (1 + 0.3 * rng.standard_normal(Q.shape).clip(-2, 2))
+        Q[0] = np.abs(Q[0]) + 0.05
+        o.write(Q)
+        o.step(30)
+    assert ref.fallback_count() == 0
