@@ -59,7 +59,7 @@ struct a3d_solver {
   double cfl = 0.7;
   int order = 2;
   long it = 0;
-  int kernel = a3d::KERNEL_TMA;      // fastest single-case stage kernel on B200
+  int kernel = a3d::KERNEL_TMA;      // the fastest single-case stage kernel measured on B200
   CUtensorMap tmQ[3];             // TMA maps over the three state buffers
   CUtensorMap tmC;                // TMA map over the code array
   int march_kz = 16;              // z planes per CTA of the marching kernels

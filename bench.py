@@ -96,7 +96,9 @@ class Clocks:
     def __init__(self, index):
         self.index = index
         self.p = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{index}.csv")
+        # raw samples; A3D_BENCH_OUT chooses the folder (default: bench_out/ in the repository)
+        out = os.environ.get("A3D_BENCH_OUT", os.path.join(ROOT, "bench_out"))
+        self.path = os.path.join(out, f"clocks_rank{index}.csv")
 
     def start(self):
         try:
