@@ -58,15 +58,14 @@ __device__ __forceinline__ Prim rot(const float P[5], int d) {
 __device__ __forceinline__ void hllc(const Prim& L, const Prim& R, float F[5]) {
   const float gL = kG * L.p, gR = kG * R.p;
   const float aL = gL * rsqrtf(gL * L.r), aR = gR * rsqrtf(gR * R.r);
-  const float EL = L.p * (1.0f / kGm) + 0.5f * L.r * (L.un * L.un + L.u1 * L.u1 + L.u2 * L.u2);
-  const float ER = R.p * (1.0f / kGm) + 0.5f * R.r * (R.un * R.un + R.u1 * R.u1 + R.u2 * R.u2);
   const float SL = fminf(L.un - aL, R.un - aR), SR = fmaxf(L.un + aL, R.un + aR);
   const float dL = SL - L.un, dR = SR - R.un;
   const float qL = L.r * dL, qR = R.r * dR;
   const float SM = __fdividef(R.p - L.p + qL * L.un - qR * R.un, qL - qR);
   const bool left = SM >= 0.f;
   const float rK = left ? L.r : R.r, uK = left ? L.un : R.un, v1 = left ? L.u1 : R.u1, v2 = left ? L.u2 : R.u2;
-  const float pK = left ? L.p : R.p, EK = left ? EL : ER;
+  const float pK = left ? L.p : R.p;
+  const float EK = pK * (1.0f / kGm) + 0.5f * rK * (uK * uK + v1 * v1 + v2 * v2);  // total energy, side K only
   const float S = left ? fminf(SL, 0.f) : fmaxf(SR, 0.f);
   const float d = left ? dL : dR, q = left ? qL : qR;
   // where S' = 0 the star terms are multiplied away; keep their divisor finite there
