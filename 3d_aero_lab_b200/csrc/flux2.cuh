@@ -44,6 +44,8 @@ __device__ __forceinline__ M1 ge0(float a) { return {a >= 0.f}; }
 __device__ __forceinline__ M2 ge0(float2 a) { return {a.x >= 0.f, a.y >= 0.f}; }
 __device__ __forceinline__ M1 le0(float a) { return {a <= 0.f}; }
 __device__ __forceinline__ M2 le0(float2 a) { return {a.x <= 0.f, a.y <= 0.f}; }
+__device__ __forceinline__ M1 ne0(float a) { return {a != 0.f}; }
+__device__ __forceinline__ M2 ne0(float2 a) { return {a.x != 0.f, a.y != 0.f}; }
 __device__ __forceinline__ M1 lor(M1 a, M1 b) { return {a.x || b.x}; }
 __device__ __forceinline__ M2 lor(M2 a, M2 b) { return {a.x || b.x, a.y || b.y}; }
 __device__ __forceinline__ float sel(M1 m, float a, float b) { return m.x ? a : b; }
@@ -61,45 +63,36 @@ __device__ __forceinline__ PrimV<T> sel(M m, const PrimV<T>& a, const PrimV<T>& 
 
 // HLLC flux through faces with left/right states L, R (already reconstructed).
 // F = {mass, normal momentum, tangential momenta, energy}.
-// Star-region flux rearranged as in flux.cuh: d = S - u_K, q = rho_K d, g = 1/(S - S_M);
-// rho* = q g, tangential fluxes v_t F_mass, E* = g (d E + (S_M - u)(q S_M + p)); sound speeds
-// g p rsqrt(g p rho) - two reciprocals and two reciprocal square roots per face.
+// Same rearrangement as flux.cuh: d = S - u_K, q = rho_K d, g = 1/(S - S_M); rho* = q g,
+// tangential fluxes v_t F_mass, E* = g (d E + (S_M - u)(q S_M + p)); the total energy on the
+// upwind side K only; sound speeds g p rsqrt(g p rho); and no supersonic branch: with the wave
+// speed clipped to S' = min(S_L, 0) left of the contact and max(S_R, 0) right of it, the star
+// formula gives the upwind state flux where the fan is supersonic (S' = 0).
 template <class T>
 __device__ __forceinline__ void hllc(const PrimV<T>& L, const PrimV<T>& R, T F[5]) {
-  const T g = splat(kG, L.r), igm = splat(1.0f / kGm, L.r), half = splat(0.5f, L.r);
+  const T g = splat(kG, L.r), igm = splat(1.0f / kGm, L.r), half = splat(0.5f, L.r), zero = splat(0.f, L.r);
+  const T one = splat(1.f, L.r);
   const T gL = mul(g, L.p), gR = mul(g, R.p);
   const T aL = mul(gL, rsqrt(mul(gL, L.r))), aR = mul(gR, rsqrt(mul(gR, R.r)));
-  const T kL = fma(L.un, L.un, fma(L.u1, L.u1, mul(L.u2, L.u2)));
-  const T kR = fma(R.un, R.un, fma(R.u1, R.u1, mul(R.u2, R.u2)));
-  const T EL = fma(L.p, igm, mul(mul(half, L.r), kL)), ER = fma(R.p, igm, mul(mul(half, R.r), kR));
   const T SL = min(sub(L.un, aL), sub(R.un, aR)), SR = max(add(L.un, aL), add(R.un, aR));
-  const T mL = mul(L.r, L.un), mR = mul(R.r, R.un);
   const T dL = sub(SL, L.un), dR = sub(SR, R.un);
   const T qL = mul(L.r, dL), qR = mul(R.r, dR);
   // contact speed SM = (pR - pL + qL uL - qR uR) / (qL - qR)
   const T SM = mul(sub(fma(qL, L.un, sub(R.p, L.p)), mul(qR, R.un)), rcp(sub(qL, qR)));
   const auto left = ge0(SM);
   const PrimV<T> K = sel(left, L, R);
-  const T S = sel(left, SL, SR), EK = sel(left, EL, ER), mK = sel(left, mL, mR);
+  const T kK = fma(K.un, K.un, fma(K.u1, K.u1, mul(K.u2, K.u2)));
+  const T EK = fma(K.p, igm, mul(mul(half, K.r), kK));
+  const T mK = mul(K.r, K.un);
+  const T SK = sel(left, SL, SR), S = sel(left, min(SL, zero), max(SR, zero));
   const T dK = sel(left, dL, dR), qK = sel(left, qL, qR);
-  const T gK = rcp(sub(S, SM));
-  T Fs[5];
-  Fs[0] = fma(S, sub(mul(qK, gK), K.r), mK);
-  Fs[1] = fma(S, fma(mul(qK, gK), SM, neg(mK)), fma(mK, K.un, K.p));
-  Fs[2] = mul(K.u1, Fs[0]);
-  Fs[3] = mul(K.u2, Fs[0]);
+  const T gK = rcp(sel(ne0(S), sub(SK, SM), one));  // S' = 0: star terms vanish, keep this finite
+  F[0] = fma(S, sub(mul(qK, gK), K.r), mK);
+  F[1] = fma(S, fma(mul(qK, gK), SM, neg(mK)), fma(mK, K.un, K.p));
+  F[2] = mul(K.u1, F[0]);
+  F[3] = mul(K.u2, F[0]);
   const T Es = mul(gK, fma(sub(SM, K.un), fma(qK, SM, K.p), mul(dK, EK)));
-  Fs[4] = fma(S, sub(Es, EK), mul(K.un, add(EK, K.p)));
-  // supersonic fan: flux of the upwind state
-  const auto supL = ge0(SL);
-  const auto sup = lor(supL, le0(SR));
-  const PrimV<T> U = sel(supL, L, R);
-  const T EU = sel(supL, EL, ER), mU = sel(supL, mL, mR);
-  F[0] = sel(sup, mU, Fs[0]);
-  F[1] = sel(sup, fma(mU, U.un, U.p), Fs[1]);
-  F[2] = sel(sup, mul(mU, U.u1), Fs[2]);
-  F[3] = sel(sup, mul(mU, U.u2), Fs[3]);
-  F[4] = sel(sup, mul(U.un, add(EU, U.p)), Fs[4]);
+  F[4] = fma(S, sub(Es, EK), mul(K.un, add(EK, K.p)));
 }
 
 // MUSCL face states of one cell along one direction: lo = P - s/2 (state on its - face),

@@ -8,7 +8,7 @@
 //   * the x face i-1/2 and the z face k+1/2 of a column are evaluated together in packed f32x2
 //     arithmetic (flux2.cuh); the y face j-1/2 alone with the same arithmetic;
 //   * the first-order fallback for a non-positive reconstructed density or pressure
-//     (src/air_cfd.js:221) is taken on a warp-uniform branch, since it is rare.
+//     (src/air_cfd.js:221) is left out: it cannot fire for these floored states (flux.cuh).
 // Per plane: [A] column primitives of plane k+2 and the plane-k tile to shared memory;
 // [B] face states, x/z fluxes; [C] y fluxes and the tile-edge faces; [D] residual and update.
 // Three CTA barriers separate A|B, B|C and C|D.
@@ -60,10 +60,8 @@ __device__ __forceinline__ void tile_states(const FusedSmem& S, int y, int x, in
 // gets exactly the numbers it would get inside a tile: results do not depend on the tiling.
 __device__ __forceinline__ void single_face(float L[5], float R[5], const float Pl[5], const float Pr[5], int d,
                                             float A, float G[5]) {
-  if (v::nonpositive(L, R)) {
-#pragma unroll
-    for (int c = 0; c < 5; c++) { L[c] = Pl[c]; R[c] = Pr[c]; }
-  }
+  (void)Pl;  // the first-order fallback cannot fire (flux.cuh, face_flux_lr, says why)
+  (void)Pr;
   float F[5], Fu[5];
   if (d == 1) {
     v::hllc(v::rotv(L, d), v::rotv(R, d), F);
@@ -217,16 +215,7 @@ __device__ __forceinline__ bool stage_tile(FusedSmem& S, const CUtensorMap* tmQp
       float xL[5], xR[5], zL[5], zR[5];
 #pragma unroll
       for (int c = 0; c < 5; c++) { xL[c] = xl[c]; xR[c] = xlo[c]; zL[c] = Zh0[c]; zR[c] = z1lo[c]; }
-      const bool fbx = v::nonpositive(xL, xR), fbz = v::nonpositive(zL, zR);
-      if (__any_sync(0xffffffffu, fbx || fbz)) {  // rare: first-order fallback
-        float Pl[5];
-        load_p(S, ty + 2, tx + 1, Pl);
-#pragma unroll
-        for (int c = 0; c < 5; c++) {
-          if (fbx) { xL[c] = Pl[c]; xR[c] = W0[c]; }
-          if (fbz) { zL[c] = W0[c]; zR[c] = W1[c]; }
-        }
-      }
+      // (no first-order fallback: it cannot fire for these floored states, see flux.cuh)
       float2 F2[5];
       v::hllc(v::pack(v::rotv(xL, 0), v::rotv(zL, 2)), v::pack(v::rotv(xR, 0), v::rotv(zR, 2)), F2);
       float Fx[5] = {F2[0].x, F2[1].x, F2[2].x, F2[3].x, F2[4].x};
