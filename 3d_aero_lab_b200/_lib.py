@@ -63,6 +63,8 @@ PROTOS = {
     "a3d_batch_step": (C.c_int, [_vp, C.c_int32]),
     "a3d_batch_sync": (C.c_int, [_vp]),
     "a3d_batch_set_schedule": (C.c_int, [_vp, C.c_int32, C.c_int32]),
+    "a3d_batch_set_mode": (C.c_int, [_vp, C.c_int32]),
+    "a3d_batch_get_mode": (C.c_int, [_vp, C.POINTER(C.c_int32)]),
     "a3d_batch_get_schedule": (C.c_int, [_vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int64)]),
     "a3d_batch_tune": (C.c_int, [_vp, C.c_int32, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
                                  C.POINTER(C.c_float)]),

@@ -279,7 +279,8 @@ class Case:
 
 
 class Batch:
-    """Many solver cases advanced together: one persistent launch per RK stage (a3d_batch_*)."""
+    """Many solver cases advanced together (a3d_batch_*): concurrent per-case launches in one
+    graph (mode 1, default) or one persistent launch per RK stage (mode 0)."""
 
     def __init__(self, solvers):
         self.solvers = list(solvers)
@@ -296,7 +297,16 @@ class Batch:
     def tune(self, trial_iters=20):
         kz, ct, ms = C.c_int32(), C.c_int32(), C.c_float()
         _lib.check(_lib.lib().a3d_batch_tune(self._h, int(trial_iters), C.byref(kz), C.byref(ct), C.byref(ms)))
-        return {"kz": kz.value, "ctas_per_sm": ct.value, "ms_per_iteration": ms.value}
+        return {"kz": kz.value, "ctas_per_sm": ct.value, "ms_per_iteration": ms.value, "mode": self.mode()}
+
+    def set_mode(self, mode):
+        """0: one persistent kernel per RK stage; 1: concurrent per-case launches in one graph."""
+        _lib.check(_lib.lib().a3d_batch_set_mode(self._h, int(mode)))
+
+    def mode(self):
+        m = C.c_int32()
+        _lib.check(_lib.lib().a3d_batch_get_mode(self._h, C.byref(m)))
+        return m.value
 
     def set_schedule(self, kz, ctas_per_sm):
         _lib.check(_lib.lib().a3d_batch_set_schedule(self._h, int(kz), int(ctas_per_sm)))

@@ -8,8 +8,9 @@
 //     the same key takes it over and starts from its converged state (src/air_cfd.js:521-537:
 //     the reference's controller re-applies conditions without a reset);
 //   * every round advances all active cases together by `chunk` iterations through one batch
-//     (one persistent launch per RK stage, batch.cu), then checks each case's FP64 density
-//     residual (src/air_cfd.js:552-555, every fluid cell) against its first one;
+//     (batch.cu: every case's own launches, concurrent in one CUDA graph), then checks each
+//     case's FP64 density residual (src/air_cfd.js:552-555, every fluid cell) against its
+//     first one;
 //   * a case that dropped by the configured ratio or reached the iteration cap gets its FP64
 //     forces and Trefftz drag and leaves; the next round already contains the newcomers;
 //   * grid sequencing (src/app_cfd.js:271-278, 398-403), when configured: a cold request first

@@ -186,8 +186,8 @@ def cpu_baseline(aero, sh, cells, iters, threads, M, alpha, delta):
 
 
 def bench_batched(aero, args, ws, rank, local):
-    """C3: seeded cases of uneven size, all advanced together (one persistent launch per RK stage,
-    CUDA graph, autotuned schedule) vs the same cases solved one after another (plain loop).
+    """C3: seeded cases of uneven size, all advanced together (concurrent per-case launches or one
+    persistent launch per RK stage, in a CUDA graph, mode and schedule autotuned) vs the same cases solved one after another (plain loop).
     The case list is sharded across ranks; solves/s are whole-job values (max time over ranks)."""
     import torch
     serve = importlib.import_module("3d_aero_lab_b200.serve")

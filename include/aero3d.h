@@ -187,11 +187,12 @@ int a3d_solver_stream(a3d_solver* s, void** stream);
 /* Blocks until all work queued on the solver's stream has finished. */
 int a3d_solver_sync(a3d_solver* s);
 
-/* ---- batched solves: many cases in one persistent launch per RK stage ------------- */
+/* ---- batched solves: many cases advanced together -------------------------------- */
 /* No counterpart in the reference (its controller runs one case).  A batch groups solver
  * objects living on one device; a3d_batch_step(n) advances every case by n SSP-RK2
- * iterations with one persistent kernel launch per stage (tiles of all cases pulled from a
- * shared queue), two iterations captured once in a CUDA graph.  Each case keeps its own
+ * iterations, two iterations captured once in a CUDA graph: either every case's own launches
+ * run concurrently (mode 1) or one persistent kernel launch per stage pulls the tiles of all
+ * cases from a shared queue (mode 0).  Each case keeps its own
  * state, forces, residual and Trefftz calls; the batch orders itself after each solver's
  * queued work and each solver's later work after the batch.                            */
 typedef struct a3d_batch a3d_batch;
@@ -199,11 +200,21 @@ int a3d_batch_create(a3d_solver* const* solvers, int32_t n, a3d_batch** out);
 int a3d_batch_destroy(a3d_batch* b);
 int a3d_batch_step(a3d_batch* b, int32_t n);
 int a3d_batch_sync(a3d_batch* b);
-/* Tile schedule: z planes per tile (kz) and persistent CTAs per SM (1 or 2). */
+/* How the batch runs its cases.  Mode 1 (default): each case's own single-case stage
+ * launches, each case on its own stream forked from the batch's, two iterations captured in
+ * one CUDA graph whose per-case branches run concurrently; every case then computes exactly
+ * what a3d_solver_step computes alone.  Mode 0: the persistent kernel above.
+ * a3d_batch_tune times both and keeps the faster.  A solver stepped or reconfigured on its
+ * own between batch steps makes the batch rebuild its table and graphs.                  */
+int a3d_batch_set_mode(a3d_batch* b, int32_t mode);
+int a3d_batch_get_mode(a3d_batch* b, int32_t* mode);
+/* Tile schedule: z planes per tile (kz) and persistent CTAs per SM (1 to 3). */
 int a3d_batch_set_schedule(a3d_batch* b, int32_t kz, int32_t ctas_per_sm);
 int a3d_batch_get_schedule(a3d_batch* b, int32_t* kz, int32_t* ctas_per_sm, int64_t* tiles);
-/* Autotuner: times every (kz, CTAs per SM) candidate for trial_iters iterations on the real
- * cases (states saved and restored), keeps the fastest; best_ms = ms per iteration.    */
+/* Autotuner: times every (kz, CTAs per SM) candidate of mode 0, then mode 1, for trial_iters
+ * iterations on the real cases (states saved and restored), keeps the fastest (best_kz and
+ * best_ctas are mode 0's best schedule; a3d_batch_get_mode tells the mode kept); best_ms =
+ * ms per iteration of the kept choice.                                                   */
 int a3d_batch_tune(a3d_batch* b, int32_t trial_iters, int32_t* best_kz, int32_t* best_ctas,
                    float* best_ms);
 

@@ -28,6 +28,7 @@ def test_batch_equals_individual_steps(aero, n, kernel):
         c.solver.set_kernel(kernel, kzs[k])
         c.solver.step(n)
     b = aero.Batch([c.solver for c in batched])
+    b.set_mode(0)  # the persistent kernel
     b.set_schedule(16, 2)
     b.step(n)
     b.sync()
@@ -40,6 +41,44 @@ def test_batch_equals_individual_steps(aero, n, kernel):
     for a, c in zip(alone, batched):
         a.solver.step(3)
         c.solver.step(3)
+        assert np.array_equal(c.solver.read_array(), a.solver.read_array())
+    # and the batch again after the solvers moved on alone (it rebuilds its case table)
+    b.step(2)
+    b.sync()
+    for a in alone:
+        a.solver.step(2)
+    for a, c in zip(alone, batched):
+        assert np.array_equal(c.solver.read_array(), a.solver.read_array())
+    b.dispose()
+
+
+@pytest.mark.parametrize("n", [21, 8])
+def test_stream_mode_equals_individual_steps(aero, n):
+    """Mode 1 (each case's own launches, concurrent in one graph): bit-identical to each case
+    stepped alone with the same stage kernel and z run, odd step counts included."""
+    alone = [make(aero, 2, *c) for c in CASES]
+    batched = [make(aero, 2, *c) for c in CASES]
+    for k in range(len(CASES)):
+        for c in (alone[k], batched[k]):
+            c.solver.set_kernel(2, (32, 64, 8, 16)[k])
+    for c in alone:
+        c.solver.step(n)
+    b = aero.Batch([c.solver for c in batched])
+    b.set_mode(1)
+    b.step(n)
+    b.sync()
+    for a, c in zip(alone, batched):
+        assert c.solver.it == a.solver.it == n
+        assert np.array_equal(c.solver.read_array(), a.solver.read_array())
+    for a, c in zip(alone, batched):  # roles carried over: both go on alike
+        a.solver.step(3)
+        c.solver.step(3)
+        assert np.array_equal(c.solver.read_array(), a.solver.read_array())
+    b.step(2)  # the batch again after the solvers moved on alone
+    b.sync()
+    for a in alone:
+        a.solver.step(2)
+    for a, c in zip(alone, batched):
         assert np.array_equal(c.solver.read_array(), a.solver.read_array())
     b.dispose()
 
@@ -65,7 +104,7 @@ def test_tuner_restores_state_and_picks_a_schedule(aero, kernel):
     before = [c.solver.read_array() for c in cases]
     b = aero.Batch([c.solver for c in cases])
     best = b.tune(4)
-    assert best["kz"] in (8, 16, 32, 64) and best["ctas_per_sm"] in ((1, 2, 3) if kernel == 2 else (1, 2)) and best["ms_per_iteration"] > 0
+    assert best["mode"] in (0, 1) and best["kz"] in (8, 16, 32, 64) and best["ctas_per_sm"] in ((1, 2, 3) if kernel == 2 else (1, 2)) and best["ms_per_iteration"] > 0
     assert b.schedule()["kz"] == best["kz"]
     for c, q in zip(cases, before):
         assert c.solver.it == 5
