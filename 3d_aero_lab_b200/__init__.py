@@ -5,8 +5,9 @@ the C ABI of include/aero3d.h (libaero3d.so, built in-tree by build.py).
 Import with importlib (the directory name starts with a digit):
     aero = importlib.import_module("3d_aero_lab_b200")
 """
-from . import abi, aircraft, engine  # noqa: F401  (pure host code, no library needed)
+from . import abi, aircraft, engine, field  # noqa: F401  (pure host code, no library needed)
 from .aircraft import build_aircraft, shape_of, trefftz_x  # noqa: F401
+from .field import fix_states  # noqa: F401
 
 
 def __getattr__(name):

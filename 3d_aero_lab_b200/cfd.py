@@ -252,10 +252,15 @@ def interp_state(coarse, fine):
 
 
 class Case:
-    """One solve: aircraft -> grid -> device geometry -> solver, set up like tools/test_cfd3.js:5-10."""
+    """One solve: aircraft -> grid -> device geometry -> solver, set up like tools/test_cfd3.js:5-10.
+
+    fixed: None or "free" - free-stream fixed states, as tools/test_cfd3.js:10 sets them;
+    "cycle" - the engine field model's states at altitude h, throttle thr and afterburner ab,
+    as the app's applyCond pushes them (src/air_cfd.js:521-533); or three explicit states.
+    """
 
     def __init__(self, aircraft_type="fighter", cells=30000, M=0.6, alpha=3.0, delta=0.0, fixed=None, device=0,
-                 ac=None, kernel=None):
+                 ac=None, kernel=None, h=0.0, thr=1.0, ab=False):
         from .aircraft import build_aircraft
         self.ac = ac if ac is not None else build_aircraft(aircraft_type)
         self.shape = shape_of(self.ac)
@@ -266,7 +271,13 @@ class Case:
             self.solver.set_kernel(kernel)
         self.F = freestream(M, alpha)
         self.solver.setFree(self.F)
-        self.solver.setFix(fixed if fixed is not None else [self.F, self.F, self.F])
+        if isinstance(fixed, str) and fixed == "cycle":
+            from .field import fix_states
+            fixed = fix_states(self.ac, h, M, alpha, thr, ab)[1]
+        elif fixed is None or (isinstance(fixed, str) and fixed == "free"):
+            fixed = [self.F, self.F, self.F]
+        self.fixed = [list(map(float, f)) for f in fixed]
+        self.solver.setFix(self.fixed)
         self.solver.reset()
         self.xT = trefftz_x(self.ac)
 

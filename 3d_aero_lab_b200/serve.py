@@ -2,7 +2,8 @@
 
 `requests(seed, n)` draws cases from the batched distribution (aircraft type uniform over the
 three default aircraft, cells U[20k, 2M], M U[0.3, 0.85], alpha U[-2, 8] deg, delta U[-5, 5]
-deg, free-stream fixed states); `Server` wraps the C scheduler; `poisson_run` submits a request
+deg, free-stream fixed states or, with fix="cycle", the engine field model's states at sea level
+and full dry throttle); `Server` wraps the C scheduler; `poisson_run` submits a request
 list at seeded Poisson arrival times and collects results; `plain_loop` solves the same list
 one request at a time with the plain solver (the reference's one-case controller), with the
 same convergence rule.
@@ -33,9 +34,10 @@ def aircraft(typ):
 
 
 def requests(seed, n, cells=(20e3, 2.0e6), mach=(0.3, 0.85), alpha=(-2.0, 8.0), delta=(-5.0, 5.0),
-             geometries=None):
+             geometries=None, fix="free"):
     """Seeded case list.  `geometries` (optional) limits the distinct (type, cells, delta) draws
-    so that repeated geometries exercise the warm start."""
+    so that repeated geometries exercise the warm start.  `fix`: "free" or "cycle" (see
+    `request_fix`); it draws no random numbers, so both give the same cases."""
     rng = np.random.default_rng(seed)
     pool = None
     if geometries:
@@ -48,8 +50,18 @@ def requests(seed, n, cells=(20e3, 2.0e6), mach=(0.3, 0.85), alpha=(-2.0, 8.0), 
         else:
             typ, c, d = TYPES[rng.integers(3)], float(rng.uniform(*cells)), float(rng.uniform(*delta))
         out.append({"type": typ, "cells": round(c), "M": float(rng.uniform(*mach)),
-                    "alpha": float(rng.uniform(*alpha)), "delta": round(d, 3)})
+                    "alpha": float(rng.uniform(*alpha)), "delta": round(d, 3), "fix": fix})
     return out
+
+
+def request_fix(r, ac, F):
+    """Fixed states of a request: the free stream, or (fix="cycle") the engine field model sampled
+    as applyCond does (src/air_cfd.js:526-533) at altitude h (default 0), throttle thr (default
+    1) and afterburner ab (default off)."""
+    if r.get("fix") == "cycle":
+        from .field import fix_states
+        return fix_states(ac, r.get("h", 0.0), r["M"], r["alpha"], r.get("thr", 1.0), r.get("ab", False))[1]
+    return [F, F, F]
 
 
 def to_request(r):
@@ -60,8 +72,9 @@ def to_request(r):
     F = freestream(r["M"], r["alpha"])
     for i in range(5):
         q.F[i] = F[i]
+    fx = request_fix(r, ac, F)
     for i in range(15):
-        q.fix[i] = F[i % 5]
+        q.fix[i] = fx[i // 5][i % 5]
     q.ref_S, q.ref_xcg, q.ref_zcg, q.ref_c = ac.ref["S"], ac.ref["xcg"], ac.ref["zcg"], ac.ref["c"]
     q.xT = trefftz_x(ac)
     q.geometry_key = hash((r["type"], r["cells"], r["delta"])) & 0xFFFFFFFFFFFFFFFF
@@ -150,7 +163,7 @@ def solve_plain(r, residual_drop=1e-3, chunk=50, max_iters=3000, device=0, kerne
     s.set_kernel(kernel, 16)
     F = freestream(r["M"], r["alpha"])
     s.setFree(F)
-    s.setFix([F, F, F])
+    s.setFix(request_fix(r, ac, F))
     s.reset()
     s.residual(1)
     res0, its, res = None, 0, None

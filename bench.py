@@ -2,7 +2,10 @@
 
 Workload (the largest single-GPU plain configuration the metric is quoted on): the fighter
 half model at ~4M cells (stretched grid ~200 x 140 x 140), M0.6, alpha 3 deg, delta 3 deg,
-free-stream fixed states, SSP-RK2 with cfl 0.7, MUSCL order 2.  One *step* is one solve:
+fixed nozzle/intake states from the 1-D cycle (the engine field model sampled as the app's
+applyCond does, sea level, full dry throttle; --fix free gives free-stream states instead),
+SSP-RK2 with cfl 0.7, MUSCL order 2.  The batched and served legs use the same source of
+fixed states.  One *step* is one solve:
 reset + ITERS iterations + the FP64 force integral.  Inputs are synthetic in the sense that
 the reference publishes no dataset; the geometry is the reference's own parametric fighter.
 
@@ -64,6 +67,10 @@ def parse():
     p.add_argument("--mach", type=float, default=WORKLOAD["M"])
     p.add_argument("--alpha", type=float, default=WORKLOAD["alpha"])
     p.add_argument("--delta", type=float, default=WORKLOAD["delta"])
+    p.add_argument("--fix", default="cycle", choices=["cycle", "free"],
+                   help="fixed states of the engine cells: the engine field model's (at --altitude, full "
+                        "dry throttle) as the app's applyCond samples them, or the free stream")
+    p.add_argument("--altitude", type=float, default=0.0, help="altitude [m] of the field-model fixed states")
     p.add_argument("--kernel", type=int, default=2)
     p.add_argument("--kz", type=int, default=16)
     p.add_argument("--cpu-sample-iters", type=int, default=2)
@@ -191,11 +198,11 @@ def bench_batched(aero, args, ws, rank, local):
     The case list is sharded across ranks; solves/s are whole-job values (max time over ranks)."""
     import torch
     serve = importlib.import_module("3d_aero_lab_b200.serve")
-    reqs = serve.requests(1, args.batch_cases)[rank::ws]
+    reqs = serve.requests(1, args.batch_cases, fix=args.fix)[rank::ws]
     cases = []
     for r in reqs:
         c = aero.Case(aircraft_type=r["type"], cells=r["cells"], M=r["M"], alpha=r["alpha"], delta=r["delta"],
-                      device=local)
+                      device=local, fixed=r["fix"])
         c.solver.set_kernel(2, 16)  # the tile the batch runs (its tuned z run may round differently)
         cases.append(c)
     cells = sum(c.g.N for c in cases)
@@ -239,7 +246,8 @@ def bench_served(aero, args, ws, rank, local):
     run to a 1e-3 density-residual drop or 3000 iterations, warm starts on repeated geometry,
     150 GB admission budget; vs the same list solved one at a time in arrival order."""
     serve = importlib.import_module("3d_aero_lab_b200.serve")
-    reqs = serve.requests(7, args.serve_requests, geometries=max(4, args.serve_requests // 3))[rank::ws]
+    reqs = serve.requests(7, args.serve_requests, geometries=max(4, args.serve_requests // 3),
+                          fix=args.fix)[rank::ws]
     sv = serve.Server(budget_gb=150.0, residual_drop=1e-3, max_active=64, chunk=50, max_iters=3000, device=local)
     res, wall = serve.poisson_run(sv, reqs, args.serve_rate / ws, seed=7 + rank)
     st = sv.stats()
@@ -285,13 +293,15 @@ def run_reference(args, ws, rank):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref
     threads = ref.max_threads()
-    sh = aero.shape_of(aero.build_aircraft(WORKLOAD["aircraft"]))
+    ac = aero.build_aircraft(WORKLOAD["aircraft"])
+    sh = aero.shape_of(ac)
     g = ref.grid(sh, args.cells)
     geo = ref.geom(sh, g, WORKLOAD["delta"])
     s = ref.CfdCPU(g, geo, threads=threads)
     F = aero.cfd.freestream(WORKLOAD["M"], WORKLOAD["alpha"])
     s.setFree(F)
-    s.setFix([F, F, F])
+    s.setFix(aero.fix_states(ac, args.altitude, WORKLOAD["M"], WORKLOAD["alpha"])[1] if args.fix == "cycle"
+             else [F, F, F])
     s.reset()
     per_step = max(1, args.cpu_sample_iters)
     for _ in range(args.warmup):
@@ -326,7 +336,8 @@ def main():
     alpha = args.alpha + 0.25 * rank  # independent case per rank
     ac = aero.build_aircraft(args.aircraft)
     sh = aero.shape_of(ac)
-    case = aero.Case(ac=ac, cells=args.cells, M=args.mach, alpha=alpha, delta=args.delta, device=local)
+    case = aero.Case(ac=ac, cells=args.cells, M=args.mach, alpha=alpha, delta=args.delta, device=local,
+                     fixed=args.fix, h=args.altitude)
     s = case.solver
     s.set_kernel(args.kernel, args.kz)
     g = case.g
@@ -414,6 +425,7 @@ def main():
                "config": {"workload": f"{args.aircraft} plain solve, {g.NX}x{g.NY}x{g.NZ} = {N} cells, "
                                       f"M{args.mach} a{args.alpha} d{args.delta}, {iters} SSP-RK2 iterations per step",
                           "cells": N, "dims": [g.NX, g.NY, g.NZ], "iterations_per_step": iters,
+                          "fixed_states": args.fix if args.fix == "free" else f"cycle at {args.altitude:g} m",
                           "kernel": {0: "cell", 1: "march", 2: "tma", 3: "fused"}[args.kernel], "march_kz": args.kz,
                           "l2": "inputs larger than L2 (three 5-component float32 states of %.0f MB each)"
                                 % (20 * N / 1e6),

@@ -12,16 +12,19 @@ REQS = [{"type": "fighter", "cells": 30000, "M": 0.6, "alpha": 3.0, "delta": 3.0
 KW = {"residual_drop": 0.1, "chunk": 25, "max_iters": 400}
 
 
-def test_results_in_the_mix_equal_results_alone(aero):
+@pytest.mark.parametrize("fix", ["free", "cycle"])
+def test_results_in_the_mix_equal_results_alone(aero, fix):
+    """fix="cycle": engine cells hold the engine field model's states (sea level, full throttle)."""
     serve = importlib.import_module("3d_aero_lab_b200.serve")
+    reqs = [dict(r, fix=fix) for r in REQS]
     sv = serve.Server(max_active=8, chunk=KW["chunk"], max_iters=KW["max_iters"], residual_drop=KW["residual_drop"],
                       warm_start=False)
-    ids = [sv.submit(r) for r in REQS]           # all arrive together and overlap on the GPU
+    ids = [sv.submit(r) for r in reqs]           # all arrive together and overlap on the GPU
     mixed = [sv.wait(i, 600) for i in ids]
     st = sv.stats()
     sv.close()
-    assert st["completed"] == len(REQS) and st["rounds"] < sum(m["iterations"] for m in mixed) / KW["chunk"]
-    for r, m in zip(REQS, mixed):
+    assert st["completed"] == len(reqs) and st["rounds"] < sum(m["iterations"] for m in mixed) / KW["chunk"]
+    for r, m in zip(reqs, mixed):
         alone = serve.solve_plain(r, **KW)
         assert m["status"] == 0 and m["iterations"] == alone["iterations"]
         for k in ("CL", "CD", "Cm", "CDi"):

@@ -57,6 +57,32 @@ def test_readme_case_matches_oracle_and_pin(aero, ref, kernel):
     assert round(fg["CL"], 4) == README_CL and round(fg["CD"], 5) == README_CD
 
 
+@pytest.mark.parametrize("typ,cells,h,M,alpha,ab", [("airliner", 30000, 11000.0, 0.78, 2.5, False),
+                                                     ("fighter", 400000, 0.0, 0.6, 3.0, True)])
+def test_engine_field_fixed_states_match_oracle(aero, ref, typ, cells, h, M, alpha, ab):
+    """Fixed states from the engine field model, as the app's applyCond pushes them: the intake
+    sink and the bypass/core jets (a hot afterburning jet on the fighter)."""
+    ac = aero.build_aircraft(typ)
+    fix = aero.fix_states(ac, h, M, alpha, 1.0, ab)[1]
+    _, sh, og, ogeo, o = oracle_case(aero, ref, typ, cells, 0.0, M=M, alpha=alpha, fix=fix)
+    g, s = gpu_case(aero, sh, cells, 0.0, M=M, alpha=alpha, kernel=2, fix=fix)
+    t = np.asarray(ogeo.t)
+    assert (t == 5).sum() > 0
+    o.step(200)
+    s.step(200)
+    Qo, Qg = o.read(), s.read_array()
+    assert np.all(np.isfinite(Qg))
+    errs = [rel_max_diff(Qg[c], Qo[c]) for c in range(5)]
+    assert all(e <= tl for e, tl in zip(errs, TOL_GPUCMP)), errs
+    for k in (3, 4, 5):  # fixed cells keep their state
+        for c in range(5):
+            assert np.all(Qg[c][t == k] == np.float32(fix[k - 3][c])), (k, c)
+    r = ac.ref
+    fg = s.forces(alpha, M, r["S"], r["xcg"], 0.0, r["c"])
+    fo = o.forces(alpha, M, r["S"], r["xcg"], 0.0, r["c"])
+    assert sig4(fg["CL"]) == sig4(fo["CL"]) and sig4(fg["CD"]) == sig4(fo["CD"])
+
+
 @pytest.mark.parametrize("kernel", [1, 2, 3])
 def test_kernels_agree(aero, kernel):
     """The tiled kernels against the per-cell one (same float32 arithmetic, other summation order)."""
