@@ -58,6 +58,14 @@ PROTOS = {
     "a3d_solver_sample": (C.c_int, [_vp, C.c_int32, _dp, _dp, _i32]),
     "a3d_solver_interp_state": (C.c_int, [_vp, _vp]),
     "a3d_solver_sync": (C.c_int, [_vp]),
+    "a3d_solver_create_shape_slab": (C.c_int, [_sp, _i32, _dp, _dp, _dp, C.c_double, C.c_double,
+                                               C.c_int32, C.c_int32, C.c_int, C.POINTER(_vp)]),
+    "a3d_solver_set_owned": (C.c_int, [_vp, C.c_int32, C.c_int32]),
+    "a3d_solver_stage": (C.c_int, [_vp, C.c_int32]),
+    "a3d_solver_copy_planes": (C.c_int, [_vp, C.c_int32, _vp, C.c_int32, C.c_int32, C.c_int32]),
+    "a3d_solver_plane_ptr": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, C.POINTER(_vp),
+                                       C.POINTER(C.c_int64)]),
+    "a3d_solver_residual_parts": (C.c_int, [_vp, _dp]),
     "a3d_batch_create": (C.c_int, [C.POINTER(_vp), C.c_int32, C.POINTER(_vp)]),
     "a3d_batch_destroy": (C.c_int, [_vp]),
     "a3d_batch_step": (C.c_int, [_vp, C.c_int32]),

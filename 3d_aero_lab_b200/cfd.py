@@ -227,6 +227,47 @@ class CfdGPU:
         _lib.check(_lib.lib().a3d_solver_residual(self._h, int(stride), C.byref(v)))
         return None if v.value < 0 else v.value
 
+    # -- z-slab decomposition (split.py) --
+    @classmethod
+    def slab(cls, g, shape, z_lo, z_hi, delta=0.0, device=0):
+        """Solver of planes [z_lo, z_hi) of the case built on the full grid g (a3d_solver_create_shape_slab)."""
+        self = cls.__new__(cls)
+        self.g = Grid(g.X.f, g.Y.f, g.Z.f[z_lo:z_hi + 1].copy(), g.h, g.core)
+        self._h = C.c_void_p()
+        _lib.check(_lib.lib().a3d_solver_create_shape_slab(C.byref(_shape(shape)), g.dims, g.X.f, g.Y.f, g.Z.f,
+                                                           float(g.h), float(delta), int(z_lo), int(z_hi),
+                                                           int(device), C.byref(self._h)))
+        self.geo = None
+        self._opt = {"cfl": 0.7, "order": 2}
+        self.F = [1.0, 0.0, 0.0, 0.0, 1 / (GAMMA * (GAMMA - 1))]
+        self.fix = [list(self.F)] * 3
+        self.host = None
+        return self
+
+    def set_owned(self, k0, k1):
+        """Planes [k0, k1) that forces, Trefftz, residual and Mach maximum cover."""
+        _lib.check(_lib.lib().a3d_solver_set_owned(self._h, int(k0), int(k1)))
+
+    def stage(self, which):
+        """One RK stage (1 or 2); stage 2 completes the iteration."""
+        _lib.check(_lib.lib().a3d_solver_stage(self._h, int(which)))
+
+    def copy_planes_from(self, src, dst_k0, src_k0, nk, which):
+        """Planes of src's current (which=0) or stage-1 (which=1) state into this solver's."""
+        _lib.check(_lib.lib().a3d_solver_copy_planes(self._h, int(dst_k0), src._h, int(src_k0), int(nk), int(which)))
+
+    def plane_ptr(self, which, c, k):
+        """(device address, floats per plane) of plane k of component c."""
+        p, n = C.c_void_p(), C.c_int64()
+        _lib.check(_lib.lib().a3d_solver_plane_ptr(self._h, int(which), int(c), int(k), C.byref(p), C.byref(n)))
+        return p.value, n.value
+
+    def residual_parts(self):
+        """(sum of squared density changes, cell count) behind the last residual()."""
+        out = np.zeros(2)
+        _lib.check(_lib.lib().a3d_solver_residual_parts(self._h, out))
+        return float(out[0]), float(out[1])
+
     def sample(self, xyz):
         """Primitive states at points (n x 3): (n x 5 array, ok flags) - cfdStencil + cfdSample."""
         xyz = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)

@@ -23,6 +23,7 @@ constexpr double kCG = 1.4;
 
 struct FlArgs {
   int NX, NY, NZ;
+  int k0, k1;  // owned planes
   const uint8_t* t;
   const float *ap0, *ap2, *Xd, *Yd, *Zd, *Xc, *Zc;
 };
@@ -32,6 +33,7 @@ __device__ __forceinline__ bool force_entry(const FlArgs& f, long q, double& cx,
   if (f.t[q] != T_FLUID) return false;
   const long NX = f.NX, NXY = NX * f.NY;
   const int i = (int)(q % NX), j = (int)((q / NX) % f.NY), k = (int)(q / NXY);
+  if (k < f.k0 || k >= f.k1) return false;
   const double axm = i > 0 ? (double)f.ap0[q - 1] : 1.0, azm = k > 0 ? (double)f.ap2[q - NXY] : 1.0;
   cx = ((double)f.ap0[q] - axm) * (double)f.Yd[j] * (double)f.Zd[k];
   cz = ((double)f.ap2[q] - azm) * (double)f.Xd[i] * (double)f.Yd[j];
@@ -104,6 +106,7 @@ __global__ void k_finalize(const double* partials, double* out) {
 struct PostArgs {
   const float* Q;  // current state, component stride Np, row pitch NXp
   long Np, N;
+  long q0, q1;     // owned cells in the reference layout: [q0, q1)
   int NX, NXp;
   const uint8_t* t;  // cell types in the reference layout
   __device__ __forceinline__ long pad(long q) const { return (q / NX) * NXp + q % NX; }
@@ -124,12 +127,12 @@ __global__ void k_forces(PostArgs p, long n, const int64_t* fq, const double* fc
   block_sum_store<3>(v, partials + blockIdx.x * 3);
 }
 
-__global__ void k_trefftz(PostArgs p, int NX, int NY, int NZ, int i0, double tx, double ca, double sa,
+__global__ void k_trefftz(PostArgs p, int NX, int NY, int k0, int k1, int i0, double tx, double ca, double sa,
                           const float* Yd, const float* Zd, double* partials) {
   double v[1] = {0};
-  const long M = (long)NY * NZ;
+  const long M = (long)NY * (k1 - k0);
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < M; e += (long)gridDim.x * blockDim.x) {
-    const int j = (int)(e % NY), k = (int)(e / NY);
+    const int j = (int)(e % NY), k = k0 + (int)(e / NY);
     double u = 0, vv = 0, w = 0, ws = 0;
     for (int di = 0; di < 2; di++) {
       const long qr = ((long)k * NY + j) * NX + i0 + di, q = ((long)k * NY + j) * p.NXp + i0 + di;
@@ -154,7 +157,7 @@ __global__ void k_residual(PostArgs p, const float* prevR, int stride, double* p
   bool bad = false;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < M; e += (long)gridDim.x * blockDim.x) {
     const long qr = e * stride, q = p.pad(qr);
-    if (p.t[qr] != T_FLUID) continue;
+    if (qr < p.q0 || qr >= p.q1 || p.t[qr] != T_FLUID) continue;
     const float r = p.Q[q];
     if (!isfinite(r)) bad = true;
     const double d = (double)r - (double)prevR[q];
@@ -171,7 +174,7 @@ __global__ void k_mach(PostArgs p, int stride, double* partials) {
   const long M = (p.N + stride - 1) / stride;
   for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < M; e += (long)gridDim.x * blockDim.x) {
     const long qr = e * stride, q = p.pad(qr);
-    if (p.t[qr] != T_FLUID) continue;
+    if (qr < p.q0 || qr >= p.q1 || p.t[qr] != T_FLUID) continue;
     const double r = p.Q[q], u = (double)p.Q[p.Np + q] / r, v = (double)p.Q[2 * p.Np + q] / r,
                  w = (double)p.Q[3 * p.Np + q] / r;
     const double pr = (kCG - 1) * ((double)p.Q[4 * p.Np + q] - 0.5 * r * (u * u + v * v + w * w));
@@ -209,12 +212,16 @@ PostArgs post_args(a3d_solver* s) {
   p.NX = s->grid.NX;
   p.NXp = s->NXp;
   p.t = s->geo.t;
+  const long NXY = (long)s->grid.NX * s->grid.NY;
+  p.q0 = s->own_k0 * NXY;
+  p.q1 = s->own_k1 * NXY;
   return p;
 }
 
 FlArgs fl_args(a3d_solver* s) {
   FlArgs f;
   f.NX = s->grid.NX; f.NY = s->grid.NY; f.NZ = s->grid.NZ;
+  f.k0 = s->own_k0; f.k1 = s->own_k1;
   f.t = s->geo.t; f.ap0 = s->geo.ap0; f.ap2 = s->geo.ap2;
   f.Xd = s->grid.Xd; f.Yd = s->grid.Yd; f.Zd = s->grid.Zd; f.Xc = s->grid.Xc; f.Zc = s->grid.Zc;
   return f;
@@ -324,7 +331,7 @@ extern "C" int a3d_solver_trefftz(a3d_solver* s, double xT, double alpha_deg, do
   const double a = alpha_deg * kDeg, Mn = std::max(M, 0.05);
   double* part = s->d_red;
   double* res = s->d_red + 4096 * 4;
-  k_trefftz<<<kRedBlocks, kRedThreads, 0, s->st>>>(post_args(s), s->grid.NX, s->grid.NY, s->grid.NZ, i0, tx,
+  k_trefftz<<<kRedBlocks, kRedThreads, 0, s->st>>>(post_args(s), s->grid.NX, s->grid.NY, s->own_k0, s->own_k1, i0, tx,
                                                    std::cos(a), std::sin(a), s->grid.Yd, s->grid.Zd, part);
   k_finalize<1><<<1, kRedThreads, 0, s->st>>>(part, res);
   A3D_CUDA(cudaGetLastError());
@@ -355,6 +362,8 @@ extern "C" int a3d_solver_residual(a3d_solver* s, int32_t stride, double* res_ou
     int flag;
     memcpy(&flag, s->h_red + 2, sizeof(int));
     res = std::sqrt(s->h_red[0] / std::max(1.0, s->h_red[1])) / (double)nIt;
+    s->res_parts[0] = s->h_red[0];
+    s->res_parts[1] = s->h_red[1];
     if (flag) { set_error("non-finite density in the state"); rc = A3D_ERR_NONFINITE; }
   }
   A3D_CUDA(cudaMemcpyAsync(s->prevR, s->buf[s->iQ], s->Np * sizeof(float), cudaMemcpyDeviceToDevice, s->st));
@@ -378,5 +387,28 @@ extern "C" int a3d_solver_mach_max(a3d_solver* s, int32_t stride, double* mmax) 
   A3D_CUDA(cudaMemcpyAsync(s->h_red, out, sizeof(double), cudaMemcpyDeviceToHost, s->st));
   A3D_CUDA(cudaStreamSynchronize(s->st));
   *mmax = std::sqrt(s->h_red[0]);
+  return A3D_OK;
+}
+
+// Planes [k0, k1) that the force list, the Trefftz plane, the residual and the Mach maximum
+// cover: a z slab's own planes, without the halo planes it shares with its neighbours.
+extern "C" int a3d_solver_set_owned(a3d_solver* s, int32_t k0, int32_t k1) {
+  clear_error();
+  A3D_ARG(s, "null solver");
+  A3D_ARG(0 <= k0 && k0 < k1 && k1 <= s->grid.NZ, "owned planes must satisfy 0 <= k0 < k1 <= NZ");
+  A3D_CUDA(cudaSetDevice(s->device));
+  A3D_CUDA(cudaStreamSynchronize(s->st));
+  s->own_k0 = k0;
+  s->own_k1 = k1;
+  if (s->fl.block) cudaFree(s->fl.block);
+  s->fl = ForceList();
+  return build_force_list(s);
+}
+
+extern "C" int a3d_solver_residual_parts(a3d_solver* s, double out[2]) {
+  clear_error();
+  A3D_ARG(s && out, "null pointer");
+  out[0] = s->res_parts[0];
+  out[1] = s->res_parts[1];
   return A3D_OK;
 }

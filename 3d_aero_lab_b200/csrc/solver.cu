@@ -217,6 +217,8 @@ int solver_finish_setup(a3d_solver* s) {
   A3D_CUDA(cudaMalloc(&s->d_flag, 16));
   A3D_CUDA(cudaMemsetAsync(s->d_flag, 0, 16, s->st));
   A3D_CUDA(cudaMalloc(&s->prevR, s->Np * sizeof(float)));
+  s->own_k0 = 0;
+  s->own_k1 = s->grid.NZ;
   A3D_TRY(build_force_list(s));
   A3D_TRY(make_tensor_maps(s));
   const double F0[5] = {1, 0, 0, 0, 1 / (kGamma * (kGamma - 1))};  // src/air_cfd.js:162
@@ -242,6 +244,12 @@ int new_solver(int device, const int32_t dims[3], const double* xf, const double
   if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) {
     delete s;
     set_error("cudaStreamCreate failed");
+    return A3D_ERR_CUDA;
+  }
+  if (cudaEventCreateWithFlags(&s->ev, cudaEventDisableTiming) != cudaSuccess) {
+    cudaStreamDestroy(s->st);
+    delete s;
+    set_error("cudaEventCreate failed");
     return A3D_ERR_CUDA;
   }
   s->N = (long)dims[0] * dims[1] * dims[2];
@@ -290,6 +298,44 @@ extern "C" int a3d_solver_create_shape(const a3d_shape* shape, const int32_t dim
   return A3D_OK;
 }
 
+// Planes [z_lo, z_hi) of the case that a3d_solver_create_shape would build on the full grid
+// `dims`: the geometry is built for the full grid in temporary device memory, and the slab
+// solver keeps its planes' geometry, the z faces zf[z_lo .. z_hi] and cells of its own.  Every
+// slab array is the full one's, cut: a slab holding two halo planes beyond the planes it owns
+// reproduces the full case's face fluxes on its owned planes once the halos are exchanged.
+extern "C" int a3d_solver_create_shape_slab(const a3d_shape* shape, const int32_t dims[3], const double* xf,
+                                            const double* yf, const double* zf, double h, double delta_deg,
+                                            int32_t z_lo, int32_t z_hi, int device, a3d_solver** out) {
+  clear_error();
+  A3D_ARG(shape && dims && zf, "null pointer");
+  A3D_ARG(0 <= z_lo && z_lo < z_hi && z_hi <= dims[2], "slab planes must satisfy 0 <= z_lo < z_hi <= NZ");
+  const int32_t sd[3] = {dims[0], dims[1], z_hi - z_lo};
+  a3d_solver* s = nullptr;
+  A3D_TRY(new_solver(device, sd, xf, yf, zf + z_lo, &s));
+  GridDev gfull;
+  GeomDev full;
+  const long NXY = (long)dims[0] * dims[1], Nfull = NXY * dims[2];
+  int rc = grid_upload(dims, xf, yf, zf, s->st, gfull);
+  if (rc == A3D_OK) rc = geom_alloc(Nfull, full);
+  if (rc == A3D_OK) rc = geom_build_device(*shape, gfull, h, delta_deg, full, s->st, nullptr, nullptr);
+  if (rc == A3D_OK) {
+    const long o = (long)z_lo * NXY, n = s->N;
+    cudaError_t e = cudaMemcpyAsync(s->geo.t, full.t + o, n, cudaMemcpyDeviceToDevice, s->st);
+    const float* src[5] = {full.phi, full.ap0, full.ap1, full.ap2, full.ap3};
+    float* dst[5] = {s->geo.phi, s->geo.ap0, s->geo.ap1, s->geo.ap2, s->geo.ap3};
+    for (int a = 0; a < 5 && e == cudaSuccess; a++)
+      e = cudaMemcpyAsync(dst[a], src[a] + o, n * sizeof(float), cudaMemcpyDeviceToDevice, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    if (e != cudaSuccess) { set_error("slab geometry: %s", cudaGetErrorString(e)); rc = A3D_ERR_CUDA; }
+  }
+  geom_free(full);
+  grid_free(gfull);
+  if (rc == A3D_OK) rc = solver_finish_setup(s);
+  if (rc != A3D_OK) { a3d_solver_destroy(s); return rc; }
+  *out = s;
+  return A3D_OK;
+}
+
 extern "C" int a3d_solver_destroy(a3d_solver* s) {
   if (!s) return A3D_OK;
   cudaSetDevice(s->device);
@@ -303,6 +349,7 @@ extern "C" int a3d_solver_destroy(a3d_solver* s) {
   if (s->fl.block) cudaFree(s->fl.block);
   geom_free(s->geo);
   grid_free(s->grid);
+  if (s->ev) cudaEventDestroy(s->ev);
   if (s->st) cudaStreamDestroy(s->st);
   delete s;
   return A3D_OK;
@@ -357,6 +404,7 @@ extern "C" int a3d_solver_step(a3d_solver* s, int32_t n) {
   clear_error();
   A3D_ARG(s, "null solver");
   A3D_ARG(n >= 0, "negative iteration count");
+  A3D_ARG(s->phase == 0, "a lone stage 1 (a3d_solver_stage) is waiting for its stage 2");
   A3D_CUDA(cudaSetDevice(s->device));
   StageArgs a1, a2;
   for (int i = 0; i < n; i++) {
@@ -368,6 +416,82 @@ extern "C" int a3d_solver_step(a3d_solver* s, int32_t n) {
     std::swap(s->iQ, s->iB);
     s->it++;
   }
+  return A3D_OK;
+}
+
+// One RK stage of an iteration, for callers that exchange halo planes between the stages:
+// which = 1 forms S1 = Q + dt R(Q); which = 2 forms B = Q/2 + (S1 + dt R(S1))/2, makes it the
+// current state and counts the iteration.  The pair is the same work as a3d_solver_step(s, 1).
+extern "C" int a3d_solver_stage(a3d_solver* s, int32_t which) {
+  clear_error();
+  A3D_ARG(s, "null solver");
+  A3D_ARG(which == 1 || which == 2, "stage must be 1 or 2");
+  A3D_ARG(which == s->phase + 1, which == 1 ? "stage 1 again before stage 2" : "stage 2 before stage 1");
+  A3D_CUDA(cudaSetDevice(s->device));
+  float *Q = s->buf[s->iQ], *S1 = s->buf[s->iS1], *B = s->buf[s->iB];
+  StageArgs a;
+  if (which == 1) {
+    fill_stage_args(s, a, Q, Q, S1, 0.f, 1.f);
+    A3D_TRY(launch_stage(s, a));
+    s->phase = 1;
+  } else {
+    fill_stage_args(s, a, S1, Q, B, 0.5f, 0.5f);
+    A3D_TRY(launch_stage(s, a));
+    std::swap(s->iQ, s->iB);
+    s->it++;
+    s->phase = 0;
+  }
+  return A3D_OK;
+}
+
+namespace {
+float* state_buffer(a3d_solver* s, int which) { return s->buf[which == 1 ? s->iS1 : s->iQ]; }
+}  // namespace
+
+// Copies planes [src_k0, src_k0 + nk) of src's current state (which = 0) or stage-1 state
+// (which = 1) into planes [dst_k0, dst_k0 + nk) of dst's buffer of the same role: the halo
+// exchange of a z-slab decomposition.  The two solvers must share NX and NY; they may live
+// on different devices (peer copy).  Stream-ordered both ways: the copy runs on dst's stream
+// after src's work so far, and src's later work waits for the copy.
+extern "C" int a3d_solver_copy_planes(a3d_solver* dst, int32_t dst_k0, a3d_solver* src, int32_t src_k0, int32_t nk,
+                                      int32_t which) {
+  clear_error();
+  A3D_ARG(dst && src && dst != src, "two distinct solvers");
+  A3D_ARG(which == 0 || which == 1, "which: 0 current state, 1 stage-1 state");
+  A3D_ARG(dst->grid.NX == src->grid.NX && dst->grid.NY == src->grid.NY, "solvers differ in NX or NY");
+  A3D_ARG(nk >= 1 && src_k0 >= 0 && src_k0 + nk <= src->grid.NZ && dst_k0 >= 0 && dst_k0 + nk <= dst->grid.NZ,
+          "plane range");
+  const long plane = (long)src->grid.NY * src->NXp;
+  const size_t bytes = (size_t)nk * plane * sizeof(float);
+  const float* sp = state_buffer(src, which) + src_k0 * plane;
+  float* dp = state_buffer(dst, which) + dst_k0 * plane;
+  A3D_CUDA(cudaSetDevice(src->device));
+  A3D_CUDA(cudaEventRecord(src->ev, src->st));
+  A3D_CUDA(cudaSetDevice(dst->device));
+  A3D_CUDA(cudaStreamWaitEvent(dst->st, src->ev, 0));
+  for (int c = 0; c < 5; c++) {
+    if (src->device == dst->device)
+      A3D_CUDA(cudaMemcpyAsync(dp + c * dst->Np, sp + c * src->Np, bytes, cudaMemcpyDeviceToDevice, dst->st));
+    else
+      A3D_CUDA(cudaMemcpyPeerAsync(dp + c * dst->Np, dst->device, sp + c * src->Np, src->device, bytes, dst->st));
+  }
+  A3D_CUDA(cudaEventRecord(dst->ev, dst->st));
+  A3D_CUDA(cudaSetDevice(src->device));
+  A3D_CUDA(cudaStreamWaitEvent(src->st, dst->ev, 0));
+  return A3D_OK;
+}
+
+// Device address of plane k of component c of the current (which = 0) or stage-1 (which = 1)
+// state; planes of one component are contiguous, `plane_floats` apart.  For exchanges that a
+// caller runs itself on the solver's stream (NCCL send/recv between ranks).
+extern "C" int a3d_solver_plane_ptr(a3d_solver* s, int32_t which, int32_t c, int32_t k, void** ptr,
+                                    int64_t* plane_floats) {
+  clear_error();
+  A3D_ARG(s && ptr && plane_floats, "null pointer");
+  A3D_ARG((which == 0 || which == 1) && c >= 0 && c < 5 && k >= 0 && k < s->grid.NZ, "which, component or plane");
+  const long plane = (long)s->grid.NY * s->NXp;
+  *ptr = state_buffer(s, which) + c * s->Np + k * plane;
+  *plane_floats = plane;
   return A3D_OK;
 }
 

@@ -70,6 +70,11 @@ struct a3d_solver {
   float* prevR = nullptr;         // density snapshot for the residual
   long prevIt = 0;
   bool havePrev = false;
+  double res_parts[2] = {0, 0};   // sum of squares and cell count of the last residual
+  // z-slab decomposition of one case (a3d_solver_create_shape_slab)
+  int phase = 0;                  // 1 between a lone stage 1 and its stage 2 (a3d_solver_stage)
+  int own_k0 = 0, own_k1 = 0;     // planes the force list and reductions cover: [own_k0, own_k1)
+  cudaEvent_t ev = nullptr;       // orders plane copies between solvers (a3d_solver_copy_planes)
 };
 
 namespace a3d {

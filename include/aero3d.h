@@ -179,13 +179,42 @@ int a3d_solver_interp_state(a3d_solver* fine, const a3d_solver* coarse);
  * kernel 1: z-marching tiles that evaluate every face once, plain loads;
  * kernel 2 (default): the same fed by a TMA plane ring, three CTAs per SM;
  * kernel 3: TMA ring, face states formed once per cell, paired f32x2 faces; results do
- *           not depend on the tiling, and the batch and server paths use this tile.
+ *           not depend on the tiling.
  * march_kz = z planes per thread block (default 16).                                  */
 int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t march_kz);
 /* The solver's CUDA stream (a cudaStream_t), for callers that time or order work on it. */
 int a3d_solver_stream(a3d_solver* s, void** stream);
 /* Blocks until all work queued on the solver's stream has finished. */
 int a3d_solver_sync(a3d_solver* s);
+
+/* ---- one case split into z slabs (several devices, or ranks) ---------------------- */
+/* No counterpart in the reference (one case, one WebGL context).  A slab solver holds the
+ * planes [z_lo, z_hi) of the case a3d_solver_create_shape builds on the full grid: its own
+ * planes plus up to two halo planes on each side shared with the neighbouring slab.  Per
+ * iteration the caller runs stage 1 on every slab, exchanges the halo planes of the stage-1
+ * state (which = 1), runs stage 2, and exchanges the halo planes of the new state
+ * (which = 0).  Restricted to its own planes (a3d_solver_set_owned), a slab's forces,
+ * Trefftz integral and residual sums add up to the full case's, and Mach maxima combine by
+ * max.                                                                                  */
+int a3d_solver_create_shape_slab(const a3d_shape* shape, const int32_t dims[3],
+                                 const double* xf, const double* yf, const double* zf,
+                                 double h, double delta_deg, int32_t z_lo, int32_t z_hi,
+                                 int device, a3d_solver** out);
+/* Planes [k0, k1) (slab-local) that forces, Trefftz, residual and Mach maximum cover.    */
+int a3d_solver_set_owned(a3d_solver* s, int32_t k0, int32_t k1);
+/* One RK stage: 1 = first stage, 2 = second stage (completes the iteration).             */
+int a3d_solver_stage(a3d_solver* s, int32_t which);
+/* Halo exchange within one process: planes of src's current (which = 0) or stage-1
+ * (which = 1) state into dst's buffer of the same role; stream-ordered on both solvers,
+ * peer copy when they live on different devices.                                        */
+int a3d_solver_copy_planes(a3d_solver* dst, int32_t dst_k0, a3d_solver* src, int32_t src_k0,
+                           int32_t nk, int32_t which);
+/* Device address of plane k of component c (planes of a component are contiguous,
+ * plane_floats apart), for exchanges the caller runs on the solver's stream (NCCL).      */
+int a3d_solver_plane_ptr(a3d_solver* s, int32_t which, int32_t c, int32_t k, void** ptr,
+                         int64_t* plane_floats);
+/* Sum of squared density changes and cell count behind the last a3d_solver_residual.     */
+int a3d_solver_residual_parts(a3d_solver* s, double out[2]);
 
 /* ---- batched solves: many cases advanced together -------------------------------- */
 /* No counterpart in the reference (its controller runs one case).  A batch groups solver
