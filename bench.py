@@ -80,6 +80,9 @@ def parse():
     p.add_argument("--serve-requests", type=int, default=32)
     p.add_argument("--serve-rate", type=float, default=20.0)
     p.add_argument("--serve-sequence", type=int, default=8)
+    p.add_argument("--split", type=int, default=0,
+                   help="also time the case cut into this many z slabs: on one GPU in one process, or "
+                        "under torchrun one slab per rank (halo planes by NCCL send/recv)")
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--no-serve", action="store_true")
     return p.parse_args()
@@ -285,6 +288,62 @@ def bench_served(aero, args, ws, rank, local):
             "max_abs_dCL_cold_vs_plain": dcl, "sequenced": seq}
 
 
+def bench_split(aero, args, ws, rank, local):
+    """The plain case cut into z slabs (two halo planes each side, exchanged after every RK stage).
+
+    One process (ws == 1): --split slabs on this GPU, halo copies between them; this measures
+    the decomposition's cost against the unsplit solve.  torchrun (ws > 1): one slab per rank,
+    halos by NCCL send/recv, forces all-reduced; strong scaling of one case.  Host clock around
+    fully synchronised work, max over ranks."""
+    import torch
+    split = importlib.import_module("3d_aero_lab_b200.split")
+    iters = args.iters
+    if ws == 1:
+        sc = split.SplitCase(args.aircraft, args.cells, args.mach, args.alpha, args.delta, slabs=args.split,
+                             devices=(local,), fixed=args.fix, h=args.altitude, kernel=args.kernel, kz=args.kz,
+                             align=args.kz)
+        N = sc.g.N
+        for _ in range(args.warmup):
+            sc.step(20)
+        sc.sync()
+        t0 = time.perf_counter()
+        sc.step(iters)
+        f = sc.forces()
+        sc.sync()
+        dt = time.perf_counter() - t0
+        sc.dispose()
+        return {"workload": f"{args.aircraft} {N} cells in {args.split} z slabs on one GPU, {iters} iterations",
+                "cell_updates_per_s": N * iters / dt, "ms_per_iteration": dt / iters * 1e3,
+                "slabs": [b["own"] for b in sc.bounds], "CL": f["CL"], "CD": f["CD"]}
+    ac = aero.build_aircraft(args.aircraft)
+    sh = aero.shape_of(ac)
+    g = aero.cfd_grid(sh, args.cells)
+    bounds = split.slab_bounds(g.NZ, ws, split.HALO, args.kz)
+    b = bounds[rank]
+    s = aero.CfdGPU.slab(g, sh, *b["stored"], delta=args.delta, device=local)
+    s.set_kernel(args.kernel, args.kz)
+    F = aero.freestream(args.mach, args.alpha)
+    s.setFree(F)
+    s.setFix(aero.fix_states(ac, args.altitude, args.mach, args.alpha)[1] if args.fix == "cycle" else [F, F, F])
+    s.set_owned(b["own"][0] - b["stored"][0], b["own"][1] - b["stored"][0])
+    s.reset()
+    d = split.DistSplit(split.GpuSlab(s, local), b, device=torch.device("cuda", local))
+    for _ in range(args.warmup):
+        d.step(20)
+    s.sync()
+    barrier(ws)
+    t0 = time.perf_counter()
+    d.step(iters)
+    f = d.forces(args.alpha, max(args.mach, 0.05), ac.ref, aero.trefftz_x(ac))
+    s.sync()
+    dt = max_over_ranks(time.perf_counter() - t0, ws)
+    barrier(ws)
+    s.dispose()
+    return {"workload": f"{args.aircraft} {g.N} cells in {ws} z slabs, one per rank, {iters} iterations",
+            "cell_updates_per_s": g.N * iters / dt, "ms_per_iteration": dt / iters * 1e3, "scaling": "strong",
+            "slabs": [x["own"] for x in bounds], "CL": f["CL"], "CD": f["CD"]}
+
+
 def run_reference(args, ws, rank):
     """--impl reference: the reference's CPU algorithm (oracle port, all host threads)."""
     if rank != 0:
@@ -396,6 +455,11 @@ def main():
     e2e_ms = max_over_ranks(t0.elapsed_time(t1) / args.steps, ws)
     s.dispose()
     extra = {}
+    if args.split:
+        try:
+            extra["split"] = bench_split(aero, args, ws, rank, local)
+        except Exception as e:
+            extra["split"] = {"error": repr(e)}
     if not args.no_batch:
         try:
             extra["batched"] = bench_batched(aero, args, ws, rank, local)
