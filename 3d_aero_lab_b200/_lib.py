@@ -66,6 +66,9 @@ PROTOS = {
     "a3d_solver_plane_ptr": (C.c_int, [_vp, C.c_int32, C.c_int32, C.c_int32, C.POINTER(_vp),
                                        C.POINTER(C.c_int64)]),
     "a3d_solver_residual_parts": (C.c_int, [_vp, _dp]),
+    "a3d_solver_set_neighbors": (C.c_int, [_vp, _vp, _vp]),
+    "a3d_solver_set_chunks": (C.c_int, [_vp, C.c_int32]),
+    "a3d_solver_sync_neighbors": (C.c_int, [_vp]),
     "a3d_batch_create": (C.c_int, [C.POINTER(_vp), C.c_int32, C.POINTER(_vp)]),
     "a3d_batch_destroy": (C.c_int, [_vp]),
     "a3d_batch_step": (C.c_int, [_vp, C.c_int32]),

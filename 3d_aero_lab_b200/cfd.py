@@ -153,6 +153,10 @@ class CfdGPU:
     def set_kernel(self, kernel, march_kz=16):
         _lib.check(_lib.lib().a3d_solver_set_kernel(self._h, int(kernel), int(march_kz)))
 
+    def set_chunks(self, chunks):
+        """Pipelined z chunks of step() (kernel 2): 0 automatic, 1 none, 2..4 chunks."""
+        _lib.check(_lib.lib().a3d_solver_set_chunks(self._h, int(chunks)))
+
     # -- reference surface --
     def setFree(self, F):
         self.F = [float(v) for v in F]
@@ -261,6 +265,15 @@ class CfdGPU:
         p, n = C.c_void_p(), C.c_int64()
         _lib.check(_lib.lib().a3d_solver_plane_ptr(self._h, int(which), int(c), int(k), C.byref(p), C.byref(n)))
         return p.value, n.value
+
+    def set_neighbors(self, lo, hi):
+        """Stage kernels push the planes lo / hi keep as halo planes into their buffers."""
+        _lib.check(_lib.lib().a3d_solver_set_neighbors(self._h, lo._h if lo is not None else None,
+                                                       hi._h if hi is not None else None))
+
+    def sync_neighbors(self):
+        """The next stage waits for the neighbours' last stages (and their pushes)."""
+        _lib.check(_lib.lib().a3d_solver_sync_neighbors(self._h))
 
     def residual_parts(self):
         """(sum of squared density changes, cell count) behind the last residual()."""

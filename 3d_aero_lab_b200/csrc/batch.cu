@@ -334,6 +334,9 @@ extern "C" int a3d_batch_create(a3d_solver* const* solvers, int32_t n, a3d_batch
   for (int k = 0; k < n; k++) {
     A3D_ARG(solvers[k], "null solver");
     A3D_ARG(solvers[k]->device == dev, "all solvers of a batch must live on one device");
+    A3D_ARG(solvers[k]->own_k0 == 0 && solvers[k]->own_k1 == solvers[k]->grid.NZ && !solvers[k]->nbr[0] &&
+                !solvers[k]->nbr[1],
+            "z-slab solvers cannot be batched");
     A3D_ARG(solvers[k]->kernel == KERNEL_FUSED || solvers[k]->kernel == KERNEL_TMA, "batch needs TMA-capable solvers");
     A3D_ARG(solvers[k]->kernel == solvers[0]->kernel, "all solvers of a batch must select the same stage kernel");
   }

@@ -19,6 +19,7 @@
 #include <vector>
 #include "flux.cuh"
 #include "solver.cuh"
+#include "store.cuh"
 
 namespace a3d {
 
@@ -80,13 +81,16 @@ __global__ void __launch_bounds__(256) k_stage_cell(StageArgs a) {
   const long q = blockIdx.x * (long)blockDim.x + threadIdx.x;
   if (q >= N) return;
   const int i = (int)(q % a.NX), j = (int)((q / a.NX) % a.NY), k = (int)(q / NXY);
+  if (k < a.kb || k >= a.ke) return;  // not one of this solver's own planes
   const long qp = ((long)k * a.NY + j) * a.NXp + i;  // padded state/code index
   const uint8_t cq = a.code[qp];
   const int t = cq & 7;
   const long Np = a.Np;
   if (t != T_FLUID) {  // src/air_cfd.js:242
-    if (t >= T_SINK) for (int c = 0; c < 5; c++) a.Out[c * Np + qp] = a.Ufix[t - T_SINK][c];
-    else for (int c = 0; c < 5; c++) a.Out[c * Np + qp] = a.B[c * Np + qp];
+    float o[5];
+    if (t >= T_SINK) for (int c = 0; c < 5; c++) o[c] = a.Ufix[t - T_SINK][c];
+    else for (int c = 0; c < 5; c++) o[c] = a.B[c * Np + qp];
+    store_out(a, a.Out, qp, k, o);
     return;
   }
   float Pc[5];
@@ -158,7 +162,7 @@ __global__ void __launch_bounds__(256) k_stage_cell(StageArgs a) {
   o[0] = fmaxf(o[0], 1e-4f);  // positivity clamps (src/air_cfd.js:247-249)
   const float ke = 0.5f * (o[1] * o[1] + o[2] * o[2] + o[3] * o[3]) / o[0];
   if (kGm * (o[4] - ke) < 1e-5f) o[4] = 1e-5f / kGm + ke;
-  for (int c = 0; c < 5; c++) a.Out[c * Np + qp] = o[c];
+  store_out(a, a.Out, qp, k, o);
 }
 
 int blocks_for(long work, int threads = 256) {
@@ -182,6 +186,30 @@ void fill_stage_args(a3d_solver* s, StageArgs& a, const float* Qin, const float*
   a.NX = s->grid.NX; a.NY = s->grid.NY; a.NZ = s->grid.NZ;
   a.wa = wa; a.wb = wb; a.cfl = (float)s->cfl; a.order2 = s->order == 2;
   a.err = s->d_flag + 1;
+  a.kb = s->own_k0;
+  a.ke = s->own_k1;
+  for (int sd = 0; sd < 2; sd++) {
+    a.peer[sd] = nullptr;
+    a.peer_np[sd] = 0;
+    a.peer_k0[sd] = a.peer_k1[sd] = a.peer_dk[sd] = 0;
+    a3d_solver* n = s->nbr[sd];
+    if (!n || !Out) continue;
+    // the neighbour's buffer of the role Out plays here; a neighbour that already finished
+    // this iteration's stage 2 has swapped its B into its current state
+    float* dst = Out == s->buf[s->iS1] ? n->buf[n->iS1]
+               : Out == s->buf[s->iB] ? (n->it > s->it ? n->buf[n->iQ] : n->buf[n->iB]) : nullptr;
+    if (!dst) continue;
+    // own planes that the neighbour stores as halo planes: its planes outside its own range
+    const int g0 = s->z_lo + s->own_k0, g1 = s->z_lo + s->own_k1;
+    const int h0 = sd == 0 ? n->z_lo + n->own_k1 : n->z_lo, h1 = sd == 0 ? n->z_lo + n->grid.NZ : n->z_lo + n->own_k0;
+    const int k0 = std::max(g0, h0), k1 = std::min(g1, h1);
+    if (k0 >= k1) continue;
+    a.peer[sd] = dst;
+    a.peer_np[sd] = n->Np;
+    a.peer_k0[sd] = k0 - s->z_lo;
+    a.peer_k1[sd] = k1 - s->z_lo;
+    a.peer_dk[sd] = s->z_lo - n->z_lo;
+  }
   prim_of(s->F, a.Pff);
   for (int f = 0; f < 3; f++) {
     prim_of(s->fix[f], a.Pfix[f]);
@@ -219,6 +247,11 @@ int solver_finish_setup(a3d_solver* s) {
   A3D_CUDA(cudaMalloc(&s->prevR, s->Np * sizeof(float)));
   s->own_k0 = 0;
   s->own_k1 = s->grid.NZ;
+  A3D_CUDA(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
+  for (int c = 0; c < 4; c++) {
+    A3D_CUDA(cudaStreamCreateWithFlags(&s->cst[c], cudaStreamNonBlocking));
+    for (int t = 0; t < 2; t++) A3D_CUDA(cudaEventCreateWithFlags(&s->cev[c][t], cudaEventDisableTiming));
+  }
   A3D_TRY(build_force_list(s));
   A3D_TRY(make_tensor_maps(s));
   const double F0[5] = {1, 0, 0, 0, 1 / (kGamma * (kGamma - 1))};  // src/air_cfd.js:162
@@ -312,6 +345,7 @@ extern "C" int a3d_solver_create_shape_slab(const a3d_shape* shape, const int32_
   const int32_t sd[3] = {dims[0], dims[1], z_hi - z_lo};
   a3d_solver* s = nullptr;
   A3D_TRY(new_solver(device, sd, xf, yf, zf + z_lo, &s));
+  s->z_lo = z_lo;
   GridDev gfull;
   GeomDev full;
   const long NXY = (long)dims[0] * dims[1], Nfull = NXY * dims[2];
@@ -350,6 +384,12 @@ extern "C" int a3d_solver_destroy(a3d_solver* s) {
   geom_free(s->geo);
   grid_free(s->grid);
   if (s->ev) cudaEventDestroy(s->ev);
+  if (s->ev_fork) cudaEventDestroy(s->ev_fork);
+  for (int c = 0; c < 4; c++) {
+    if (s->cst[c]) cudaStreamDestroy(s->cst[c]);
+    for (int t = 0; t < 2; t++)
+      if (s->cev[c][t]) cudaEventDestroy(s->cev[c][t]);
+  }
   if (s->st) cudaStreamDestroy(s->st);
   delete s;
   return A3D_OK;
@@ -400,12 +440,81 @@ extern "C" int a3d_solver_reset(a3d_solver* s) {
   return A3D_OK;
 }
 
+namespace {
+
+// Number of pipelined z chunks a3d_solver_step uses: kernel 2 on a whole case only.  Automatic:
+// four chunks from 1M cells up (a stage then takes about 50 us, which hides the extra stream
+// and event calls; measured on the 4.1M-cell fighter 13.5 -> 15.0 G cell-updates/s, on a 1.2M
+// one 9.25 -> 9.45), none below (host-bound there).
+int chunk_count(const a3d_solver* s) {
+  if (s->kernel != KERNEL_TMA || s->nbr[0] || s->nbr[1] || s->own_k0 != 0 || s->own_k1 != s->grid.NZ) return 1;
+  const int runs = (s->grid.NZ + s->march_kz - 1) / s->march_kz;
+  const int K = s->chunks_req > 0 ? s->chunks_req : (s->N >= 1000000 ? 4 : 1);
+  return std::max(1, std::min(K, std::min(runs, 4)));
+}
+
+// n iterations with the case cut into K z chunks of whole z runs (so every cell sees the same
+// arithmetic as in one launch).  Chunk c's stage waits for the previous stage of chunks c-1 and
+// c+1 only: a stage reads two planes beyond its chunk and writes inside it, so those are its
+// only producers (read after write) and its only remaining readers (write after read).
+int step_chunked(a3d_solver* s, int n, int K) {
+  const int kz = s->march_kz, NZ = s->grid.NZ, runs = (NZ + kz - 1) / kz;
+  int kb[4], ke[4];
+  for (int c = 0; c < K; c++) {
+    kb[c] = (c * runs / K) * kz;
+    ke[c] = std::min(NZ, ((c + 1) * runs / K) * kz);
+  }
+  A3D_CUDA(cudaEventRecord(s->ev_fork, s->st));
+  for (int c = 0; c < K; c++) A3D_CUDA(cudaStreamWaitEvent(s->cst[c], s->ev_fork, 0));
+  bool first = true;
+  for (int i = 0; i < n; i++) {
+    float *Q = s->buf[s->iQ], *S1 = s->buf[s->iS1], *B = s->buf[s->iB];
+    for (int stage = 0; stage < 2; stage++) {
+      StageArgs a;
+      if (stage == 0) fill_stage_args(s, a, Q, Q, S1, 0.f, 1.f);
+      else fill_stage_args(s, a, S1, Q, B, 0.5f, 0.5f);
+      const int qin_buf = a.Qin == s->buf[0] ? 0 : a.Qin == s->buf[1] ? 1 : 2;
+      const int prev = stage ^ 1;
+      for (int c = 0; c < K; c++) {
+        if (!first) {
+          if (c > 0) A3D_CUDA(cudaStreamWaitEvent(s->cst[c], s->cev[c - 1][prev], 0));
+          if (c + 1 < K) A3D_CUDA(cudaStreamWaitEvent(s->cst[c], s->cev[c + 1][prev], 0));
+        }
+        a.kb = kb[c];
+        a.ke = ke[c];
+        A3D_TRY(launch_tma(s, a, qin_buf, stage == 1, s->cst[c]));
+        A3D_CUDA(cudaEventRecord(s->cev[c][stage], s->cst[c]));
+      }
+      first = false;
+    }
+    std::swap(s->iQ, s->iB);
+    s->it++;
+  }
+  for (int c = 0; c < K; c++) A3D_CUDA(cudaStreamWaitEvent(s->st, s->cev[c][1], 0));
+  return A3D_OK;
+}
+
+}  // namespace
+
+// Pipelined z chunks of a3d_solver_step (kernel 2): 0 = automatic (4 from 1M cells up, else 1),
+// 1 = one launch per stage, 2..4 = that many chunks.  Results do not depend on it.
+extern "C" int a3d_solver_set_chunks(a3d_solver* s, int32_t chunks) {
+  clear_error();
+  A3D_ARG(s, "null solver");
+  A3D_ARG(chunks >= 0 && chunks <= 4, "chunks must be 0 (automatic) or 1..4");
+  s->chunks_req = chunks;
+  return A3D_OK;
+}
+
 extern "C" int a3d_solver_step(a3d_solver* s, int32_t n) {
   clear_error();
   A3D_ARG(s, "null solver");
   A3D_ARG(n >= 0, "negative iteration count");
   A3D_ARG(s->phase == 0, "a lone stage 1 (a3d_solver_stage) is waiting for its stage 2");
+  A3D_ARG(!s->nbr[0] && !s->nbr[1], "a slab with neighbours advances by a3d_solver_stage");
   A3D_CUDA(cudaSetDevice(s->device));
+  const int K = chunk_count(s);
+  if (K > 1 && n > 0) return step_chunked(s, n, K);
   StageArgs a1, a2;
   for (int i = 0; i < n; i++) {
     float *Q = s->buf[s->iQ], *S1 = s->buf[s->iS1], *B = s->buf[s->iB];
@@ -427,6 +536,14 @@ extern "C" int a3d_solver_stage(a3d_solver* s, int32_t which) {
   A3D_ARG(s, "null solver");
   A3D_ARG(which == 1 || which == 2, "stage must be 1 or 2");
   A3D_ARG(which == s->phase + 1, which == 1 ? "stage 1 again before stage 2" : "stage 2 before stage 1");
+  for (a3d_solver* n : s->nbr) {
+    if (!n) continue;
+    // the neighbour is at the same stage of the same iteration, before or after its own launch
+    const bool ok = which == 1 ? n->it == s->it
+                               : ((n->it == s->it && n->phase == 1) || (n->it == s->it + 1 && n->phase == 0));
+    A3D_ARG(ok, "neighbour slabs out of step");
+    A3D_ARG(s->kernel == KERNEL_CELL || s->kernel == KERNEL_TMA, "halo push needs stage kernel 0 or 2");
+  }
   A3D_CUDA(cudaSetDevice(s->device));
   float *Q = s->buf[s->iQ], *S1 = s->buf[s->iS1], *B = s->buf[s->iB];
   StageArgs a;
@@ -441,6 +558,48 @@ extern "C" int a3d_solver_stage(a3d_solver* s, int32_t which) {
     s->it++;
     s->phase = 0;
   }
+  if (s->nbr[0] || s->nbr[1]) A3D_CUDA(cudaEventRecord(s->ev, s->st));
+  return A3D_OK;
+}
+
+// Makes s's stage kernels also store the planes that its neighbours keep as halo planes
+// straight into the neighbours' buffers (peer stores when they live on other devices), so
+// that no copy is needed between stages.  lo / hi: the slabs below and above (either may be
+// null).  Every slab of the split must be given its neighbours; afterwards a slab advances
+// by a3d_solver_stage, with a3d_solver_sync_neighbors between the stages of all slabs.
+// Kernels 0 and 2 store only own planes and push; others are refused.
+extern "C" int a3d_solver_set_neighbors(a3d_solver* s, a3d_solver* lo, a3d_solver* hi) {
+  clear_error();
+  A3D_ARG(s && s != lo && s != hi, "null or self neighbour");
+  A3D_ARG(s->kernel == KERNEL_CELL || s->kernel == KERNEL_TMA, "halo push needs stage kernel 0 or 2");
+  for (a3d_solver* n : {lo, hi}) {
+    if (!n) continue;
+    A3D_ARG(n->grid.NX == s->grid.NX && n->grid.NY == s->grid.NY, "neighbour differs in NX or NY");
+    A3D_ARG(n->it == s->it && n->phase == 0 && s->phase == 0, "neighbours must be at the same iteration");
+    if (n->device != s->device) {
+      int can = 0;
+      A3D_CUDA(cudaDeviceCanAccessPeer(&can, s->device, n->device));
+      A3D_ARG(can, "no peer access between the slabs' devices");
+      A3D_CUDA(cudaSetDevice(s->device));
+      const cudaError_t e = cudaDeviceEnablePeerAccess(n->device, 0);
+      if (e == cudaErrorPeerAccessAlreadyEnabled) cudaGetLastError();
+      else A3D_CUDA(e);
+    }
+  }
+  if (lo) A3D_ARG(lo->z_lo < s->z_lo, "lower neighbour must start below");
+  if (hi) A3D_ARG(hi->z_lo > s->z_lo, "upper neighbour must start above");
+  s->nbr[0] = lo;
+  s->nbr[1] = hi;
+  return A3D_OK;
+}
+
+// s's next stage waits until its neighbours' last stages (and their pushes into s) are done.
+extern "C" int a3d_solver_sync_neighbors(a3d_solver* s) {
+  clear_error();
+  A3D_ARG(s, "null solver");
+  A3D_CUDA(cudaSetDevice(s->device));
+  for (a3d_solver* n : s->nbr)
+    if (n) A3D_CUDA(cudaStreamWaitEvent(s->st, n->ev, 0));
   return A3D_OK;
 }
 

@@ -28,6 +28,12 @@ struct StageArgs {
   float Pfix[3][5];               // primitive fixed states of types 3, 4, 5
   float Ufix[3][5];               // conservative fixed states written to fixed cells
   int* err;                       // set when a bounded wait inside a stage kernel ran out
+  // z slabs (kernels 0 and 2): planes this launch computes and stores, and the halo push
+  int kb, ke;                     // [kb, ke): the solver's own planes (all planes unless split)
+  float* peer[2];                 // lower/upper neighbour slab's buffer of the output role, or null
+  long peer_np[2];                // its component stride
+  int peer_k0[2], peer_k1[2];     // own planes [k0, k1) that are the neighbour's halo planes
+  int peer_dk[2];                 // the neighbour's plane index = own plane index + peer_dk
 };
 
 // Device-side force-list entry arrays (cfdForceList).
@@ -73,8 +79,16 @@ struct a3d_solver {
   double res_parts[2] = {0, 0};   // sum of squares and cell count of the last residual
   // z-slab decomposition of one case (a3d_solver_create_shape_slab)
   int phase = 0;                  // 1 between a lone stage 1 and its stage 2 (a3d_solver_stage)
-  int own_k0 = 0, own_k1 = 0;     // planes the force list and reductions cover: [own_k0, own_k1)
-  cudaEvent_t ev = nullptr;       // orders plane copies between solvers (a3d_solver_copy_planes)
+  int own_k0 = 0, own_k1 = 0;     // own planes: the ones stage kernels store and reductions cover
+  int z_lo = 0;                   // global index of the slab's plane 0
+  a3d_solver* nbr[2] = {nullptr, nullptr};  // lower/upper neighbour slab the stage kernels push to
+  cudaEvent_t ev = nullptr;       // orders plane copies and pushes between solvers
+  // pipelined z chunks of a3d_solver_step (kernel 2): chunk c's stages run on stream cst[c] and
+  // wait only for chunks c-1 and c+1, so one stage's tail overlaps the next stage's start
+  int chunks_req = 0;             // 0: automatic
+  cudaStream_t cst[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaEvent_t cev[4][2] = {};
+  cudaEvent_t ev_fork = nullptr;
 };
 
 namespace a3d {
@@ -83,7 +97,7 @@ int launch_stage(a3d_solver* s, const StageArgs& a);
 void fill_stage_args(a3d_solver* s, StageArgs& a, const float* Qin, const float* B, float* Out, float wa, float wb);
 int build_force_list(a3d_solver* s);
 int make_tensor_maps(a3d_solver* s);
-int launch_tma(a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2);
+int launch_tma(a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2, cudaStream_t st = nullptr);
 int launch_fused(a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2);
 size_t fused_smem_bytes();
 size_t tma_smem_bytes();

@@ -9,14 +9,32 @@ namespace {
 
 using namespace tma;
 
-// 80 registers without spills: three CTAs (24 warps) per SM.
-template <bool STAGE2>
+// 80 registers without spills: three CTAs (24 warps) per SM.  MODE 0: all planes of the case;
+// 1: planes [a.kb, a.ke) (a z chunk or a slab's own planes); 2: the same with the halo push of
+// a z slab.  Separate instances, so that the whole-case kernel carries none of it.
+template <bool STAGE2, int MODE>
 __global__ void __launch_bounds__(TX * TY, 3)
     k_stage_tma(const __grid_constant__ CUtensorMap tmQ, const __grid_constant__ CUtensorMap tmC, StageArgs a,
                 int kz) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   TmaSmem& S = *reinterpret_cast<TmaSmem*>(smem_raw);
-  stage_tile<STAGE2, false>(S, &tmQ, &tmC, a, a.B, a.Out, blockIdx.x, blockIdx.y, blockIdx.z, kz);
+  stage_tile<STAGE2, false, MODE >= 1, MODE == 2>(S, &tmQ, &tmC, a, a.B, a.Out, blockIdx.x, blockIdx.y, blockIdx.z,
+                                                  kz);
+}
+
+template <bool STAGE2, int MODE>
+int set_tma_attributes() {
+  A3D_CUDA(cudaFuncSetAttribute(k_stage_tma<STAGE2, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)tma_smem_bytes()));
+  A3D_CUDA(cudaFuncSetAttribute(k_stage_tma<STAGE2, MODE>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  return A3D_OK;
+}
+
+template <int MODE>
+void launch_mode(const a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2, dim3 grid, cudaStream_t st) {
+  const size_t sm = tma_smem_bytes();
+  if (stage2) k_stage_tma<true, MODE><<<grid, TX * TY, sm, st>>>(s->tmQ[qin_buf], s->tmC, a, s->march_kz);
+  else k_stage_tma<false, MODE><<<grid, TX * TY, sm, st>>>(s->tmQ[qin_buf], s->tmC, a, s->march_kz);
 }
 
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -55,20 +73,23 @@ int make_tensor_maps(a3d_solver* s) {
                    CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) { set_error("cuTensorMapEncodeTiled(codes) failed: %d", (int)r); return A3D_ERR_CUDA; }
   // kernel attributes are per device: set them on every solver's device
-  A3D_CUDA(cudaFuncSetAttribute(k_stage_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem_bytes()));
-  A3D_CUDA(cudaFuncSetAttribute(k_stage_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem_bytes()));
-  A3D_CUDA(cudaFuncSetAttribute(k_stage_tma<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
-  A3D_CUDA(cudaFuncSetAttribute(k_stage_tma<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100));
+  A3D_TRY((set_tma_attributes<false, 0>()));
+  A3D_TRY((set_tma_attributes<true, 0>()));
+  A3D_TRY((set_tma_attributes<false, 1>()));
+  A3D_TRY((set_tma_attributes<true, 1>()));
+  A3D_TRY((set_tma_attributes<false, 2>()));
+  A3D_TRY((set_tma_attributes<true, 2>()));
   return fused_set_attributes();
 }
 
-int launch_tma(a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2) {
+// The stage kernel over planes [a.kb, a.ke) on stream st (the solver's stream by default).
+int launch_tma(a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2, cudaStream_t st) {
   const int kz = s->march_kz;
-  dim3 grid((a.NX + TX - 1) / TX, (a.NY + TY - 1) / TY, (a.NZ + kz - 1) / kz);
-  if (stage2)
-    k_stage_tma<true><<<grid, TX * TY, tma_smem_bytes(), s->st>>>(s->tmQ[qin_buf], s->tmC, a, kz);
-  else
-    k_stage_tma<false><<<grid, TX * TY, tma_smem_bytes(), s->st>>>(s->tmQ[qin_buf], s->tmC, a, kz);
+  dim3 grid((a.NX + TX - 1) / TX, (a.NY + TY - 1) / TY, (a.ke - a.kb + kz - 1) / kz);
+  if (!st) st = s->st;
+  if (a.peer[0] || a.peer[1]) launch_mode<2>(s, a, qin_buf, stage2, grid, st);
+  else if (a.kb != 0 || a.ke != a.NZ) launch_mode<1>(s, a, qin_buf, stage2, grid, st);
+  else launch_mode<0>(s, a, qin_buf, stage2, grid, st);
   A3D_CUDA(cudaGetLastError());
   return A3D_OK;
 }

@@ -18,6 +18,7 @@
 #include <cudaTypedefs.h>
 #include "flux.cuh"
 #include "solver.cuh"
+#include "store.cuh"
 #include "tma.cuh"
 #include "tma_ring.cuh"
 
@@ -108,14 +109,17 @@ __device__ __forceinline__ float face_z_carry(const StageArgs& a, const float Lb
 // bounded wait ran out (flagged in *a.err); the CTA's copies in flight are then drained.
 // PERSISTENT: the CTA runs further tiles after this one (batch kernel), so the tile starts with
 // a barrier and retires its ring barriers at the end.
-template <bool STAGE2, bool PERSISTENT>
+// RANGE: the z runs cover planes [a.kb, a.ke) only (a z slab's own planes, or one z chunk of a
+// pipelined step).  PUSH: a cell store also goes to a neighbour slab that keeps the plane as a
+// halo plane (store_out).
+template <bool STAGE2, bool PERSISTENT, bool RANGE = false, bool PUSH = false>
 __device__ __forceinline__ bool stage_tile(TmaSmem& S, const CUtensorMap* tmQ, const CUtensorMap* tmC,
                                            const StageArgs& a, const float* __restrict__ Bp,
                                            float* __restrict__ Outp, int bx, int by, int bz, int kz) {
   const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
   const int i0 = bx * TX, j0 = by * TY;
   const int i = i0 + tx, j = j0 + ty;
-  const int k0 = bz * kz, k1 = min(a.NZ, k0 + kz);
+  const int k0 = RANGE ? a.kb + bz * kz : bz * kz, k1 = RANGE ? min(a.ke, k0 + kz) : min(a.NZ, k0 + kz);
   const bool in_dom = i < a.NX && j < a.NY;
   const long NXY = (long)a.NX * a.NY, Np = a.Np;
   const float rx = in_dom ? a.rXd[i] : 0.f, ry = in_dom ? a.rYd[j] : 0.f;
@@ -301,8 +305,12 @@ __device__ __forceinline__ bool stage_tile(TmaSmem& S, const CUtensorMap* tmQ, c
         const float ke = 0.5f * (o[1] * o[1] + o[2] * o[2] + o[3] * o[3]) / o[0];
         if (kGm * (o[4] - ke) < 1e-5f) o[4] = 1e-5f / kGm + ke;
       }
+      if (PUSH) {
+        store_out(a, Outp, qp, k, o);
+      } else {
 #pragma unroll
-      for (int c = 0; c < 5; c++) Outp[c * Np + qp] = o[c];
+        for (int c = 0; c < 5; c++) Outp[c * Np + qp] = o[c];
+      }
     }
 #pragma unroll
     for (int c = 0; c < 5; c++) { Gz[c] = Gn[c]; Lz[c] = Ln[c]; W0[c] = W1[c]; W1[c] = W2[c]; }

@@ -17,8 +17,11 @@ cross-plane face fluxes, the local time step and the wall source.  Halo planes a
 too and then overwritten.  Forces, the Trefftz integral and the residual sums are restricted
 to own planes and add up across slabs; Mach maxima combine by max.
 
-`SplitCase` drives the slabs from one process with `a3d_solver_copy_planes`, a peer copy
-when neighbours live on different devices.  `DistSplit` runs one slab per rank of a
+`SplitCase` drives the slabs from one process.  By default the stage kernels push: each
+slab's stage kernel stores the planes its neighbours keep as halo planes straight into their
+buffers, peer stores over NVLink when they live on other devices.  Stream waits on the
+neighbours' events then order the next stage, and no copy runs between stages.  With
+push=False the halos move by `a3d_solver_copy_planes` after each stage instead.  `DistSplit` runs one slab per rank of a
 torch.distributed group.  It exchanges the halo planes with point-to-point send/recv on the
 solver's stream (NCCL over NVLink for CUDA ranks) and all-reduces the force and residual sums.
 """
@@ -34,9 +37,9 @@ HALO = 2
 def slab_bounds(NZ, n, halo=HALO, align=1):
     """Own ranges [a, b) and stored ranges [lo, hi) (own plus halos) of n z slabs.
 
-    Interior boundaries sit near i NZ / n.  align > 1 moves each of them so that the slab
-    above it starts its stored range (boundary - halo) on a multiple of align.  That way a
-    z-marching tile of align planes starts its runs where the unsplit solve starts them.
+    Interior boundaries sit near i NZ / n.  align > 1 rounds each to a multiple of align.
+    The stage kernels run over a slab's own planes, so a z-marching tile of align planes then
+    starts its runs where the unsplit solve starts them.
     """
     if n < 1:
         raise ValueError("need at least one slab")
@@ -44,7 +47,7 @@ def slab_bounds(NZ, n, halo=HALO, align=1):
     for i in range(1, n):
         b = int(round(i * NZ / n))
         if align > 1:
-            b = int(round((b - halo) / align)) * align + halo
+            b = int(round(b / align)) * align
         cuts.append(b)
     cuts.append(NZ)
     for i in range(n):
@@ -62,7 +65,7 @@ class SplitCase:
     """A case on z slabs driven from one process (the slabs may live on several devices)."""
 
     def __init__(self, aircraft_type="fighter", cells=30000, M=0.6, alpha=3.0, delta=0.0, slabs=2, devices=(0,),
-                 fixed=None, h=0.0, thr=1.0, ab=False, kernel=None, kz=16, align=1, ac=None):
+                 fixed=None, h=0.0, thr=1.0, ab=False, kernel=None, kz=16, align=1, ac=None, push=True):
         from .aircraft import build_aircraft, trefftz_x
         from .cfd import CfdGPU, cfd_grid, freestream, shape_of
         self.ac = ac if ac is not None else build_aircraft(aircraft_type)
@@ -88,6 +91,11 @@ class SplitCase:
             s.set_owned(b["own"][0] - lo, b["own"][1] - lo)
             s.reset()
             self.slabs.append(s)
+        self.push = push
+        if push:
+            for n, s in enumerate(self.slabs):
+                s.set_neighbors(self.slabs[n - 1] if n > 0 else None,
+                                self.slabs[n + 1] if n + 1 < len(self.slabs) else None)
         self.xT = trefftz_x(self.ac)
         self.it = 0
         self._res_it = None
@@ -103,12 +111,14 @@ class SplitCase:
 
     def step(self, n):
         for _ in range(int(n)):
-            for s in self.slabs:
-                s.stage(1)
-            self._exchange(1)
-            for s in self.slabs:
-                s.stage(2)
-            self._exchange(0)
+            for which in (1, 2):
+                for s in self.slabs:
+                    s.stage(which)
+                if self.push:
+                    for s in self.slabs:
+                        s.sync_neighbors()
+                else:
+                    self._exchange(1 if which == 1 else 0)
             self.it += 1
 
     def sync(self):

@@ -182,6 +182,11 @@ int a3d_solver_interp_state(a3d_solver* fine, const a3d_solver* coarse);
  *           not depend on the tiling.
  * march_kz = z planes per thread block (default 16).                                  */
 int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t march_kz);
+/* Kernel 2 steps the case as up to 4 z chunks of whole z runs on their own streams, each
+ * chunk's stage waiting only for its neighbour chunks' previous stage: the tail of one stage
+ * overlaps the start of the next.  0 = automatic (4 chunks from 1M cells up, else 1),
+ * 1 = one launch per stage, 2..4 = that many chunks.  The results are the same bit for bit. */
+int a3d_solver_set_chunks(a3d_solver* s, int32_t chunks);
 /* The solver's CUDA stream (a cudaStream_t), for callers that time or order work on it. */
 int a3d_solver_stream(a3d_solver* s, void** stream);
 /* Blocks until all work queued on the solver's stream has finished. */
@@ -213,6 +218,13 @@ int a3d_solver_copy_planes(a3d_solver* dst, int32_t dst_k0, a3d_solver* src, int
  * plane_floats apart), for exchanges the caller runs on the solver's stream (NCCL).      */
 int a3d_solver_plane_ptr(a3d_solver* s, int32_t which, int32_t c, int32_t k, void** ptr,
                          int64_t* plane_floats);
+/* Halo push instead of copies: s's stage kernels also store the own planes that its lower
+ * and upper neighbours (either may be NULL) keep as halo planes into the neighbours' buffers,
+ * peer stores across devices.  Afterwards s advances only by a3d_solver_stage; call
+ * a3d_solver_sync_neighbors on every slab after every stage of all slabs, so that each slab's
+ * next stage waits for its neighbours' stores.  Stage kernels 0 and 2.                   */
+int a3d_solver_set_neighbors(a3d_solver* s, a3d_solver* lo, a3d_solver* hi);
+int a3d_solver_sync_neighbors(a3d_solver* s);
 /* Sum of squared density changes and cell count behind the last a3d_solver_residual.     */
 int a3d_solver_residual_parts(a3d_solver* s, double out[2]);
 

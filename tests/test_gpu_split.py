@@ -20,13 +20,17 @@ def full_case(aero, typ, cells, M, alpha, delta, kernel, fixed):
     return c
 
 
+@pytest.mark.parametrize("push", [True, False])
 @pytest.mark.parametrize("kernel,slabs,align,exact", [(0, 2, 1, True), (0, 3, 1, True), (2, 3, 16, True),
                                                       (2, 2, 1, False)])
-def test_slabs_reproduce_the_unsplit_solve(aero, kernel, slabs, align, exact):
+def test_slabs_reproduce_the_unsplit_solve(aero, kernel, slabs, align, exact, push):
+    """push: stage kernels store the neighbours' halo planes into their buffers; otherwise the
+    halos are copied between the stages."""
     split = importlib_split()
     typ, cells, M, alpha, delta = "fighter", 400000, 0.6, 3.0, 3.0
     full = full_case(aero, typ, cells, M, alpha, delta, kernel, "cycle")
-    sc = split.SplitCase(typ, cells, M, alpha, delta, slabs=slabs, kernel=kernel, kz=16, align=align, fixed="cycle")
+    sc = split.SplitCase(typ, cells, M, alpha, delta, slabs=slabs, kernel=kernel, kz=16, align=align, fixed="cycle",
+                         push=push)
     assert len(sc.slabs) == slabs and sc.g.N == full.g.N
     assert full.solver.residual(1) is None and sc.residual(1) is None
     full.solver.step(30)
@@ -44,6 +48,29 @@ def test_slabs_reproduce_the_unsplit_solve(aero, kernel, slabs, align, exact):
     assert math.isclose(sc.trefftz(), full.trefftz(), rel_tol=1e-9 if exact else 1e-5)
     assert math.isclose(sc.residual(1), full.solver.residual(1), rel_tol=1e-9 if exact else 1e-4)
     assert math.isclose(sc.mach_max(1), full.solver.mach_max(1), rel_tol=1e-12 if exact else 1e-5)
+    sc.dispose()
+
+
+def test_pushing_slabs_refuse_unordered_use(aero):
+    split = importlib_split()
+    sc = split.SplitCase("fighter", 60000, 0.6, 3.0, 0.0, slabs=2, kernel=2)
+    s0, s1 = sc.slabs
+    with pytest.raises(aero.AeroError):
+        s0.step(1)                                  # a pushing slab advances by stages only
+    s0.stage(1)
+    with pytest.raises(aero.AeroError):
+        s0.stage(1)                                 # stage 1 twice
+    with pytest.raises(aero.AeroError):
+        s1.stage(2)                                 # stage 2 before its stage 1
+    s1.stage(1)
+    s0.sync_neighbors()
+    s1.sync_neighbors()
+    s0.stage(2)
+    s1.stage(2)
+    with pytest.raises(aero.AeroError):
+        aero.Batch([s0, s1])                        # slab solvers are not batched
+    with pytest.raises(aero.AeroError):
+        s0.set_kernel(1, 16) or s0.stage(1)         # the march kernel cannot push
     sc.dispose()
 
 

@@ -38,7 +38,7 @@ def test_slab_bounds_cover_the_planes_once():
             (a, e), (lo, hi) = x["own"], x["stored"]
             assert e - a >= split.HALO and lo == max(0, a - 2) and hi == min(NZ, e + 2)
             if align > 1 and i > 0:
-                assert lo % align == 0
+                assert a % align == 0
     with pytest.raises(ValueError):
         split.slab_bounds(5, 4)
 
