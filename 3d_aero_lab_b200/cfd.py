@@ -157,6 +157,12 @@ class CfdGPU:
         """Pipelined z chunks of step() (kernel 2): 0 automatic, 1 none, 2..4 chunks."""
         _lib.check(_lib.lib().a3d_solver_set_chunks(self._h, int(chunks)))
 
+    def chunks(self):
+        """Stage launches per RK stage that step() uses for this case."""
+        v = C.c_int32()
+        _lib.check(_lib.lib().a3d_solver_get_chunks(self._h, C.byref(v)))
+        return v.value
+
     # -- reference surface --
     def setFree(self, F):
         self.F = [float(v) for v in F]

@@ -506,6 +506,14 @@ extern "C" int a3d_solver_set_chunks(a3d_solver* s, int32_t chunks) {
   return A3D_OK;
 }
 
+// The number of z chunks a3d_solver_step would use now (stage launches per stage).
+extern "C" int a3d_solver_get_chunks(a3d_solver* s, int32_t* chunks) {
+  clear_error();
+  A3D_ARG(s && chunks, "null pointer");
+  *chunks = chunk_count(s);
+  return A3D_OK;
+}
+
 extern "C" int a3d_solver_step(a3d_solver* s, int32_t n) {
   clear_error();
   A3D_ARG(s, "null solver");

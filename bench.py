@@ -14,7 +14,9 @@ e2e    - the same through the public solver API with host buffers: each step upl
          initial state from pinned memory, solves, reads the full state back and computes
          the forces (CUDA events around the whole sequence on the solver stream).
 roofline.achieved - 142 algorithmic bytes per cell-update (stage 1: read Q + metadata 41 B,
-         write S1 20 B; stage 2: read S1, Q and metadata 61 B, write B 20 B) x cell-updates/s.
+         write S1 20 B; stage 2: read S1, Q and metadata 61 B, write B 20 B) x cell-updates/s
+         of the stage kernels alone: 71 B x N per RK stage (all of its z-chunk launches) over
+         the stage time measured with CUDA events on the solver's stream.
 
 --impl reference times the reference's CPU algorithm instead (the C++ restatement of CfdCPU,
 OpenMP over all host cores): the JavaScript original cannot run on this machine.
@@ -403,7 +405,8 @@ def main():
     N = g.N
     stream = torch.cuda.ExternalStream(s.stream, device=torch.device("cuda", local))
     iters = args.iters
-    launches_per_step = 1 + 2 * iters + 2  # reset fill, two stages per iteration, force reduction
+    chunks = s.chunks()  # pipelined z chunks: stage launches per RK stage
+    launches_per_step = 1 + 2 * iters * chunks + 2  # reset fill, stage launches, force reduction
 
     def solve():
         s.reset()
@@ -491,6 +494,7 @@ def main():
                           "cells": N, "dims": [g.NX, g.NY, g.NZ], "iterations_per_step": iters,
                           "fixed_states": args.fix if args.fix == "free" else f"cycle at {args.altitude:g} m",
                           "kernel": {0: "cell", 1: "march", 2: "tma", 3: "fused"}[args.kernel], "march_kz": args.kz,
+                          "z_chunks": chunks,
                           "l2": "inputs larger than L2 (three 5-component float32 states of %.0f MB each)"
                                 % (20 * N / 1e6),
                           "parallelism": f"{ws} independent solves (one per GPU)" if ws > 1 else "single GPU"},

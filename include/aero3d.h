@@ -187,6 +187,8 @@ int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t march_kz);
  * overlaps the start of the next.  0 = automatic (4 chunks from 1M cells up, else 1),
  * 1 = one launch per stage, 2..4 = that many chunks.  The results are the same bit for bit. */
 int a3d_solver_set_chunks(a3d_solver* s, int32_t chunks);
+/* The number of chunks (stage launches per RK stage) a3d_solver_step uses for this case.  */
+int a3d_solver_get_chunks(a3d_solver* s, int32_t* chunks);
 /* The solver's CUDA stream (a cudaStream_t), for callers that time or order work on it. */
 int a3d_solver_stream(a3d_solver* s, void** stream);
 /* Blocks until all work queued on the solver's stream has finished. */
