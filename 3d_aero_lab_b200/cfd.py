@@ -150,8 +150,15 @@ class CfdGPU:
             self._opt["order"] = int(order)
         _lib.check(_lib.lib().a3d_solver_set_opt(self._h, self._opt["cfl"], self._opt["order"]))
 
-    def set_kernel(self, kernel, march_kz=16):
+    def set_kernel(self, kernel, march_kz=0):
+        """Stage kernel and z planes per CTA (0: picked from the grid size)."""
         _lib.check(_lib.lib().a3d_solver_set_kernel(self._h, int(kernel), int(march_kz)))
+
+    def kernel(self):
+        """(stage kernel, z planes per CTA) in use."""
+        k, kz = C.c_int32(), C.c_int32()
+        _lib.check(_lib.lib().a3d_solver_get_kernel(self._h, C.byref(k), C.byref(kz)))
+        return k.value, kz.value
 
     def set_chunks(self, chunks):
         """Pipelined z chunks of step() (kernel 2): 0 automatic, 1 none, 2..4 chunks."""

@@ -287,7 +287,7 @@ void scheduler(a3d_server* sv) {
       }
       int32_t kz0 = 0, ct0 = 0;  // keep the batch's default CTAs per SM for its tile
       a3d_batch_get_schedule(batch, &kz0, &ct0, nullptr);
-      a3d_batch_set_schedule(batch, sv->cfg.kz, ct0);
+      a3d_batch_set_schedule(batch, sv->cfg.kz > 0 ? sv->cfg.kz : kz0, ct0);
       batch_key = key;
     }
     int rc = a3d_batch_step(batch, sv->cfg.chunk_iters);
@@ -345,7 +345,7 @@ extern "C" int a3d_server_create(const a3d_server_config* cfg, a3d_server** out)
   A3D_TRY(use_device(cfg->device));
   a3d_server* sv = new a3d_server();
   sv->cfg = *cfg;
-  if (sv->cfg.kz <= 0) sv->cfg.kz = 16;
+  if (sv->cfg.kz < 0) sv->cfg.kz = 0;  // 0: each case picks its z run (a3d_solver_set_kernel)
   sv->t0 = Clock::now();
   sv->th = std::thread(scheduler, sv);
   *out = sv;

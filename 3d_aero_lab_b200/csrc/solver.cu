@@ -254,6 +254,7 @@ int solver_finish_setup(a3d_solver* s) {
   }
   A3D_TRY(build_force_list(s));
   A3D_TRY(make_tensor_maps(s));
+  A3D_TRY(a3d_solver_set_kernel(s, s->kernel, 0));  // the automatic z run
   const double F0[5] = {1, 0, 0, 0, 1 / (kGamma * (kGamma - 1))};  // src/air_cfd.js:162
   for (int c = 0; c < 5; c++) { s->F[c] = F0[c]; s->fix[0][c] = s->fix[1][c] = s->fix[2][c] = F0[c]; }
   A3D_CUDA(cudaStreamSynchronize(s->st));
@@ -443,13 +444,13 @@ extern "C" int a3d_solver_reset(a3d_solver* s) {
 namespace {
 
 // Number of pipelined z chunks a3d_solver_step uses: kernel 2 on a whole case only.  Automatic:
-// four chunks from 1M cells up (a stage then takes about 50 us, which hides the extra stream
-// and event calls; measured on the 4.1M-cell fighter 13.5 -> 15.0 G cell-updates/s, on a 1.2M
-// one 9.25 -> 9.45), none below (host-bound there).
+// four chunks from 0.8M cells up, where a stage takes long enough to hide the extra stream and
+// event calls (measured: 4.1M-cell fighter 13.5 -> 15.1 G cell-updates/s, 1.0M-cell airliner
+// 10.1 -> 11.2), none below (0.6M-cell interceptor 8.4 -> 8.1 with four).
 int chunk_count(const a3d_solver* s) {
   if (s->kernel != KERNEL_TMA || s->nbr[0] || s->nbr[1] || s->own_k0 != 0 || s->own_k1 != s->grid.NZ) return 1;
   const int runs = (s->grid.NZ + s->march_kz - 1) / s->march_kz;
-  const int K = s->chunks_req > 0 ? s->chunks_req : (s->N >= 1000000 ? 4 : 1);
+  const int K = s->chunks_req > 0 ? s->chunks_req : (s->N >= 800000 ? 4 : 1);
   return std::max(1, std::min(K, std::min(runs, 4)));
 }
 
@@ -496,7 +497,7 @@ int step_chunked(a3d_solver* s, int n, int K) {
 
 }  // namespace
 
-// Pipelined z chunks of a3d_solver_step (kernel 2): 0 = automatic (4 from 1M cells up, else 1),
+// Pipelined z chunks of a3d_solver_step (kernel 2): 0 = automatic (4 from 0.8M cells up, else 1),
 // 1 = one launch per stage, 2..4 = that many chunks.  Results do not depend on it.
 extern "C" int a3d_solver_set_chunks(a3d_solver* s, int32_t chunks) {
   clear_error();
@@ -698,15 +699,36 @@ extern "C" int a3d_solver_write(a3d_solver* s, const float* r, const float* ru, 
   return A3D_OK;
 }
 
-// Selects the stage kernel (0: per-cell, 1: z-march) and the march's z planes per CTA.
-// Not part of the reference surface; used by the parity tests and the autotuner.
+// Selects the stage kernel (0: per-cell, 1: z-march, 2: TMA, 3: fused) and the z planes per
+// CTA of the tiled kernels.  march_kz = 0 picks it: 16, unless the TMA tile would then launch
+// fewer than two waves of CTAs (tiles x z runs < 2 x resident CTAs), where 8 keeps the SMs
+// busy and the z chunks of a3d_solver_step overlapping (measured on a 1.5M-cell fighter,
+// 217 x 76 x 91: 11.4 -> 13.8 G cell-updates/s).  Not part of the reference surface.
 extern "C" int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t march_kz) {
   clear_error();
   A3D_ARG(s, "null solver");
   A3D_ARG(kernel >= KERNEL_CELL && kernel <= KERNEL_FUSED, "kernel");
-  A3D_ARG(march_kz >= 1 && march_kz <= 1024, "march_kz");
+  A3D_ARG(march_kz >= 0 && march_kz <= 1024, "march_kz");
+  if (march_kz == 0) {
+    march_kz = 16;
+    if (kernel == KERNEL_TMA) {
+      const long tiles = (long)((s->grid.NX + 31) / 32) * ((s->grid.NY + 7) / 8) * ((s->grid.NZ + 15) / 16);
+      int resident = 0;
+      A3D_CUDA(cudaSetDevice(s->device));
+      A3D_TRY(tma_resident_ctas(&resident));
+      if (tiles < 2L * resident) march_kz = 8;
+    }
+  }
   s->kernel = kernel;
   s->march_kz = march_kz;
+  return A3D_OK;
+}
+
+extern "C" int a3d_solver_get_kernel(a3d_solver* s, int32_t* kernel, int32_t* march_kz) {
+  clear_error();
+  A3D_ARG(s && kernel && march_kz, "null pointer");
+  *kernel = s->kernel;
+  *march_kz = s->march_kz;
   return A3D_OK;
 }
 

@@ -101,6 +101,7 @@ int launch_tma(a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2, cuda
 int launch_fused(a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2);
 size_t fused_smem_bytes();
 size_t tma_smem_bytes();
+int tma_resident_ctas(int* n);          // CTAs of the TMA stage kernel resident on the current device
 int fused_set_attributes();
 int check_kernel_error(a3d_solver* s);  // A3D_ERR_TIMEOUT if a stage kernel flagged a timeout
 }  // namespace a3d

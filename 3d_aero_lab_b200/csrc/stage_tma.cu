@@ -53,6 +53,16 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 size_t tma_smem_bytes() { return sizeof(TmaSmem) + 128; }
 
+int tma_resident_ctas(int* n) {
+  int dev = 0, sms = 0, per_sm = 0;
+  A3D_CUDA(cudaGetDevice(&dev));
+  A3D_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  A3D_TRY((set_tma_attributes<false, 1>()));
+  A3D_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_stage_tma<false, 1>, TX * TY, tma_smem_bytes()));
+  *n = sms * std::max(1, per_sm);
+  return A3D_OK;
+}
+
 // Tensor maps over the padded state buffers (x, y, z, component) and the code array (x, y, z).
 int make_tensor_maps(a3d_solver* s) {
   auto enc = encode_fn();

@@ -74,7 +74,7 @@ def parse():
                         "dry throttle) as the app's applyCond samples them, or the free stream")
     p.add_argument("--altitude", type=float, default=0.0, help="altitude [m] of the field-model fixed states")
     p.add_argument("--kernel", type=int, default=2)
-    p.add_argument("--kz", type=int, default=16)
+    p.add_argument("--kz", type=int, default=0, help="z planes per CTA; 0 picks from the grid size")
     p.add_argument("--cpu-sample-iters", type=int, default=2)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--batch-cases", type=int, default=64)
@@ -208,7 +208,7 @@ def bench_batched(aero, args, ws, rank, local):
     for r in reqs:
         c = aero.Case(aircraft_type=r["type"], cells=r["cells"], M=r["M"], alpha=r["alpha"], delta=r["delta"],
                       device=local, fixed=r["fix"])
-        c.solver.set_kernel(2, 16)  # the tile the batch runs (its tuned z run may round differently)
+        c.solver.set_kernel(2, 0)  # the tile and z run the batch's per-case launches use
         cases.append(c)
     cells = sum(c.g.N for c in cases)
     it = args.batch_iters
@@ -406,6 +406,7 @@ def main():
     stream = torch.cuda.ExternalStream(s.stream, device=torch.device("cuda", local))
     iters = args.iters
     chunks = s.chunks()  # pipelined z chunks: stage launches per RK stage
+    kz_used = s.kernel()[1]
     launches_per_step = 1 + 2 * iters * chunks + 2  # reset fill, stage launches, force reduction
 
     def solve():
@@ -493,7 +494,7 @@ def main():
                                       f"M{args.mach} a{args.alpha} d{args.delta}, {iters} SSP-RK2 iterations per step",
                           "cells": N, "dims": [g.NX, g.NY, g.NZ], "iterations_per_step": iters,
                           "fixed_states": args.fix if args.fix == "free" else f"cycle at {args.altitude:g} m",
-                          "kernel": {0: "cell", 1: "march", 2: "tma", 3: "fused"}[args.kernel], "march_kz": args.kz,
+                          "kernel": {0: "cell", 1: "march", 2: "tma", 3: "fused"}[args.kernel], "march_kz": kz_used,
                           "z_chunks": chunks,
                           "l2": "inputs larger than L2 (three 5-component float32 states of %.0f MB each)"
                                 % (20 * N / 1e6),

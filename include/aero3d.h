@@ -180,11 +180,13 @@ int a3d_solver_interp_state(a3d_solver* fine, const a3d_solver* coarse);
  * kernel 2 (default): the same fed by a TMA plane ring, three CTAs per SM;
  * kernel 3: TMA ring, face states formed once per cell, paired f32x2 faces; results do
  *           not depend on the tiling.
- * march_kz = z planes per thread block (default 16).                                  */
+ * march_kz = z planes per thread block; 0 (the default) picks 16, or 8 where the TMA tile
+ * would launch fewer than two waves of CTAs.                                          */
 int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t march_kz);
+int a3d_solver_get_kernel(a3d_solver* s, int32_t* kernel, int32_t* march_kz);
 /* Kernel 2 steps the case as up to 4 z chunks of whole z runs on their own streams, each
  * chunk's stage waiting only for its neighbour chunks' previous stage: the tail of one stage
- * overlaps the start of the next.  0 = automatic (4 chunks from 1M cells up, else 1),
+ * overlaps the start of the next.  0 = automatic (4 chunks from 0.8M cells up, else 1),
  * 1 = one launch per stage, 2..4 = that many chunks.  The results are the same bit for bit. */
 int a3d_solver_set_chunks(a3d_solver* s, int32_t chunks);
 /* The number of chunks (stage launches per RK stage) a3d_solver_step uses for this case.  */
@@ -279,7 +281,7 @@ typedef struct a3d_server_config {
   int32_t max_iters;           /* iteration cap per request                             */
   int32_t device;
   int32_t warm_start;          /* 1: keep finished cases resident for reuse              */
-  int32_t kz;                  /* batch tile depth (z planes); 0: default               */
+  int32_t kz;                  /* z planes per tile; 0: each case picks its own         */
   /* Grid sequencing (the reference's setupCFD, src/app_cfd.js:271-278, 398-403): a cold
    * request first solves a coarse case of cells/sequence cells until its residual dropped by
    * sequence_drop or it ran sequence_max_iters iterations, then starts the requested case
