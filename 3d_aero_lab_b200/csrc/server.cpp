@@ -107,6 +107,15 @@ void make_room(a3d_server* sv, size_t need) {
 }
 
 // The coarse case of a sequenced request: cells / sequence, same shape and delta, free stream.
+// The per-case stage configuration of served cases: the TMA tile with the configured z run and
+// one launch per stage.  The cases already run concurrently in the server's batch, so the z
+// chunks that speed up a lone case only add launches here.
+int configure_case(a3d_server* sv, a3d_solver* s) {
+  int rc = a3d_solver_set_kernel(s, a3d::KERNEL_TMA, sv->cfg.kz);
+  if (rc == A3D_OK) rc = a3d_solver_set_chunks(s, 1);
+  return rc;
+}
+
 int start_coarse(a3d_server* sv, Job& j) {
   const a3d_request& r = j.req;
   std::vector<double> xf(16384), yf(16384), zf(16384);
@@ -121,6 +130,7 @@ int start_coarse(a3d_server* sv, Job& j) {
   rc = a3d_solver_create_shape(&r.shape, dims, xf.data(), yf.data(), zf.data(), h, r.delta_deg, sv->cfg.device,
                                &j.coarse);
   if (rc != A3D_OK) return rc;
+  configure_case(sv, j.coarse);
   sv->resident += bytes;
   j.coarse_bytes = bytes;
   a3d_solver_set_free(j.coarse, r.F);
@@ -144,7 +154,7 @@ void drop_coarse(a3d_server* sv, Job& j) {
 int switch_to_target(a3d_server* sv, Job& j) {
   j.coarse_its = j.coarse->it;
   const int chunk = sv->cfg.chunk_iters;
-  int rc = a3d_solver_set_kernel(j.s, a3d::KERNEL_TMA, sv->cfg.kz);
+  int rc = configure_case(sv, j.s);
   if (rc == A3D_OK) rc = a3d_solver_step(j.s, chunk);
   double r0 = -1, dummy;
   if (rc == A3D_OK) rc = a3d_solver_residual(j.s, 1, &r0);
@@ -176,6 +186,7 @@ int start_case(a3d_server* sv, Job& j) {
     rc = a3d_solver_create_shape(&r.shape, dims, xf.data(), yf.data(), zf.data(), h, r.delta_deg, sv->cfg.device,
                                  &j.s);
     if (rc != A3D_OK) return rc;
+    configure_case(sv, j.s);
     sv->resident += j.bytes;
   }
   a3d_solver_set_free(j.s, r.F);
@@ -345,7 +356,7 @@ extern "C" int a3d_server_create(const a3d_server_config* cfg, a3d_server** out)
   A3D_TRY(use_device(cfg->device));
   a3d_server* sv = new a3d_server();
   sv->cfg = *cfg;
-  if (sv->cfg.kz < 0) sv->cfg.kz = 0;  // 0: each case picks its z run (a3d_solver_set_kernel)
+  if (sv->cfg.kz <= 0) sv->cfg.kz = 16;
   sv->t0 = Clock::now();
   sv->th = std::thread(scheduler, sv);
   *out = sv;

@@ -87,7 +87,7 @@ def result_dict(o):
 
 class Server:
     def __init__(self, budget_gb=150.0, residual_drop=1e-3, max_active=64, chunk=50, max_iters=3000, device=0,
-                 warm_start=True, kz=0, sequence=0, sequence_drop=0.05, sequence_max_iters=1500):
+                 warm_start=True, kz=16, sequence=0, sequence_drop=0.05, sequence_max_iters=1500):
         """sequence: grid sequencing factor (a cold request first solves cells/sequence cells,
         until its residual dropped by sequence_drop or sequence_max_iters; 0 = off)."""
         cfg = a3d_server_config(budget_gb * 1e9, residual_drop, max_active, chunk, max_iters, device,
@@ -154,13 +154,16 @@ def latency_stats(res):
             "mean_s": float(lat.mean()), "max_s": float(lat.max())}
 
 
-def solve_plain(r, residual_drop=1e-3, chunk=50, max_iters=3000, device=0, kernel=2):
-    """One request on its own solver, the same convergence rule as the server.  Kernel 2 (TMA)
-    is the tile the server's batches run, so the two give bit-identical results."""
+def solve_plain(r, residual_drop=1e-3, chunk=50, max_iters=3000, device=0, kernel=2, kz=0, chunks=0):
+    """One request on its own solver, the same convergence rule as the server.  By default the
+    lone case's fastest configuration (z run and z chunks picked from its size); with the
+    server's per-case configuration (kz=16, chunks=1) the results equal the served ones bit for
+    bit."""
     ac, sh = aircraft(r["type"])
     g = cfd_grid(sh, r["cells"])
     s = CfdGPU(g, shape=sh, delta=r["delta"], device=device)
-    s.set_kernel(kernel, 0)
+    s.set_kernel(kernel, kz)
+    s.set_chunks(chunks)
     F = freestream(r["M"], r["alpha"])
     s.setFree(F)
     s.setFix(request_fix(r, ac, F))

@@ -208,7 +208,7 @@ def bench_batched(aero, args, ws, rank, local):
     for r in reqs:
         c = aero.Case(aircraft_type=r["type"], cells=r["cells"], M=r["M"], alpha=r["alpha"], delta=r["delta"],
                       device=local, fixed=r["fix"])
-        c.solver.set_kernel(2, 0)  # the tile and z run the batch's per-case launches use
+        c.solver.set_kernel(2, 0)  # plain loop: each lone case's fastest z run and z chunks
         cases.append(c)
     cells = sum(c.g.N for c in cases)
     it = args.batch_iters
@@ -222,7 +222,10 @@ def bench_batched(aero, args, ws, rank, local):
         plain.append(c.forces())
     torch.cuda.synchronize()
     t_plain = max_over_ranks(time.perf_counter() - t0, ws)
-    # batched
+    # batched: the cases run concurrently, so each keeps one launch per stage and the 16-plane run
+    for c in cases:
+        c.solver.set_kernel(2, 16)
+        c.solver.set_chunks(1)
     b = aero.Batch([c.solver for c in cases])
     tuned = b.tune(4)
     for c in cases:
