@@ -248,7 +248,7 @@ int solver_finish_setup(a3d_solver* s) {
   s->own_k0 = 0;
   s->own_k1 = s->grid.NZ;
   A3D_CUDA(cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
-  for (int c = 0; c < 4; c++) {
+  for (int c = 0; c < kMaxChunks; c++) {
     A3D_CUDA(cudaStreamCreateWithFlags(&s->cst[c], cudaStreamNonBlocking));
     for (int t = 0; t < 2; t++) A3D_CUDA(cudaEventCreateWithFlags(&s->cev[c][t], cudaEventDisableTiming));
   }
@@ -386,7 +386,7 @@ extern "C" int a3d_solver_destroy(a3d_solver* s) {
   grid_free(s->grid);
   if (s->ev) cudaEventDestroy(s->ev);
   if (s->ev_fork) cudaEventDestroy(s->ev_fork);
-  for (int c = 0; c < 4; c++) {
+  for (int c = 0; c < kMaxChunks; c++) {
     if (s->cst[c]) cudaStreamDestroy(s->cst[c]);
     for (int t = 0; t < 2; t++)
       if (s->cev[c][t]) cudaEventDestroy(s->cev[c][t]);
@@ -451,7 +451,7 @@ int chunk_count(const a3d_solver* s) {
   if (s->kernel != KERNEL_TMA || s->nbr[0] || s->nbr[1] || s->own_k0 != 0 || s->own_k1 != s->grid.NZ) return 1;
   const int runs = (s->grid.NZ + s->march_kz - 1) / s->march_kz;
   const int K = s->chunks_req > 0 ? s->chunks_req : (s->N >= 800000 ? 4 : 1);
-  return std::max(1, std::min(K, std::min(runs, 4)));
+  return std::max(1, std::min(K, std::min(runs, kMaxChunks)));
 }
 
 // n iterations with the case cut into K z chunks of whole z runs (so every cell sees the same
@@ -460,7 +460,7 @@ int chunk_count(const a3d_solver* s) {
 // only producers (read after write) and its only remaining readers (write after read).
 int step_chunked(a3d_solver* s, int n, int K) {
   const int kz = s->march_kz, NZ = s->grid.NZ, runs = (NZ + kz - 1) / kz;
-  int kb[4], ke[4];
+  int kb[kMaxChunks], ke[kMaxChunks];
   for (int c = 0; c < K; c++) {
     kb[c] = (c * runs / K) * kz;
     ke[c] = std::min(NZ, ((c + 1) * runs / K) * kz);
@@ -502,7 +502,7 @@ int step_chunked(a3d_solver* s, int n, int K) {
 extern "C" int a3d_solver_set_chunks(a3d_solver* s, int32_t chunks) {
   clear_error();
   A3D_ARG(s, "null solver");
-  A3D_ARG(chunks >= 0 && chunks <= 4, "chunks must be 0 (automatic) or 1..4");
+  A3D_ARG(chunks >= 0 && chunks <= kMaxChunks, "chunks must be 0 (automatic) or 1..4");
   s->chunks_req = chunks;
   return A3D_OK;
 }

@@ -45,6 +45,7 @@ struct ForceList {
 };
 
 enum StageKernel { KERNEL_CELL = 0, KERNEL_MARCH = 1, KERNEL_TMA = 2, KERNEL_FUSED = 3 };
+constexpr int kMaxChunks = 4;  // z chunks of a pipelined step (6 or 8 measured no faster)
 
 }  // namespace a3d
 
@@ -86,8 +87,8 @@ struct a3d_solver {
   // pipelined z chunks of a3d_solver_step (kernel 2): chunk c's stages run on stream cst[c] and
   // wait only for chunks c-1 and c+1, so one stage's tail overlaps the next stage's start
   int chunks_req = 0;             // 0: automatic
-  cudaStream_t cst[4] = {nullptr, nullptr, nullptr, nullptr};
-  cudaEvent_t cev[4][2] = {};
+  cudaStream_t cst[a3d::kMaxChunks] = {};
+  cudaEvent_t cev[a3d::kMaxChunks][2] = {};
   cudaEvent_t ev_fork = nullptr;
 };
 
