@@ -41,11 +41,11 @@ KERNEL_NAMES = {0: "k_stage_cell", 1: "k_stage_march", 2: "k_stage_tma", 3: "k_s
 
 
 def measured_traffic(kernel, cells):
-    """DRAM bytes per stage launch from the committed ncu summary (profiles/), scaled to `cells`.
+    """DRAM bytes per RK stage from the committed ncu summary (profiles/), scaled to `cells`.
 
     The summary lists, per kernel, `traffic <kernel> <bytes per cell-stage>` measured as
-    dram__bytes_read.sum + dram__bytes_write.sum of single launches on the 4.13M-cell fighter
-    (mean of a stage-1 and a stage-2 launch)."""
+    dram__bytes_read.sum + dram__bytes_write.sum on the 4.13M-cell fighter, summed over the four
+    z-chunk launches of a stage (mean of stage 1 and stage 2)."""
     path = os.path.join(ROOT, "profiles", "stage_kernels_fighter4M.md")
     if not os.path.exists(path):
         return None
