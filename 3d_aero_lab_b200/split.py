@@ -81,21 +81,25 @@ class SplitCase:
             fixed = [self.F, self.F, self.F]
         self.fixed = fixed
         self.slabs = []
-        for n, b in enumerate(self.bounds):
-            lo, hi = b["stored"]
-            s = CfdGPU.slab(self.g, self.shape, lo, hi, delta=delta, device=devices[n % len(devices)])
-            if kernel is not None:
-                s.set_kernel(kernel, kz)
-            s.setFree(self.F)
-            s.setFix(fixed)
-            s.set_owned(b["own"][0] - lo, b["own"][1] - lo)
-            s.reset()
-            self.slabs.append(s)
         self.push = push
-        if push:
-            for n, s in enumerate(self.slabs):
-                s.set_neighbors(self.slabs[n - 1] if n > 0 else None,
-                                self.slabs[n + 1] if n + 1 < len(self.slabs) else None)
+        try:
+            for n, b in enumerate(self.bounds):
+                lo, hi = b["stored"]
+                s = CfdGPU.slab(self.g, self.shape, lo, hi, delta=delta, device=devices[n % len(devices)])
+                self.slabs.append(s)
+                if kernel is not None:
+                    s.set_kernel(kernel, kz)
+                s.setFree(self.F)
+                s.setFix(fixed)
+                s.set_owned(b["own"][0] - lo, b["own"][1] - lo)
+                s.reset()
+            if push:
+                for n, s in enumerate(self.slabs):
+                    s.set_neighbors(self.slabs[n - 1] if n > 0 else None,
+                                    self.slabs[n + 1] if n + 1 < len(self.slabs) else None)
+        except Exception:
+            self.dispose()
+            raise
         self.xT = trefftz_x(self.ac)
         self.it = 0
         self._res_it = None
