@@ -85,3 +85,19 @@ def test_no_device_fails_loudly_without_fallback(aero):
     assert e.value.status == 8
     with pytest.raises(L.AeroError):
         aero.CfdGPU(g, shape=sh)
+
+
+def test_slab_and_chunk_entry_points_check_their_arguments():
+    """The z-chunk and z-slab entry points refuse null handles with a status, on any machine."""
+    from importlib import import_module
+    L = import_module("3d_aero_lab_b200._lib")
+    lib = L.lib()
+    i32 = C.c_int32()
+    calls = [lib.a3d_solver_set_chunks(None, 0), lib.a3d_solver_get_chunks(None, C.byref(i32)),
+             lib.a3d_solver_get_kernel(None, C.byref(i32), C.byref(i32)), lib.a3d_solver_stage(None, 1),
+             lib.a3d_solver_set_owned(None, 0, 1), lib.a3d_solver_copy_planes(None, 0, None, 0, 1, 0),
+             lib.a3d_solver_set_neighbors(None, None, None), lib.a3d_solver_sync_neighbors(None),
+             lib.a3d_solver_residual_parts(None, np.zeros(2))]
+    for rc in calls:
+        assert rc != 0
+        assert lib.a3d_last_error()
