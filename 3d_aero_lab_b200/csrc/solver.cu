@@ -700,10 +700,12 @@ extern "C" int a3d_solver_write(a3d_solver* s, const float* r, const float* ru, 
 }
 
 // Selects the stage kernel (0: per-cell, 1: z-march, 2: TMA, 3: fused) and the z planes per
-// CTA of the tiled kernels.  march_kz = 0 picks it: 16, unless the TMA tile would then launch
-// fewer than two waves of CTAs (tiles x z runs < 2 x resident CTAs), where 8 keeps the SMs
-// busy and the z chunks of a3d_solver_step overlapping (measured on a 1.5M-cell fighter,
-// 217 x 76 x 91: 11.4 -> 13.8 G cell-updates/s).  Not part of the reference surface.
+// CTA of the tiled kernels.  march_kz = 0 picks it for the TMA tile: the longest run of 16, 8 or
+// 4 planes that still launches two waves of CTAs (column tiles x z runs >= 2 x resident CTAs),
+// else 2.  Shorter runs cost more ring prologue per plane but keep the SMs busy and the z chunks
+// of a3d_solver_step overlapping.  Measured (G cell-updates/s, fighter): 4.1M cells 16 planes
+// 15.1; 2.0M 8 planes 13.5 (16: 12.2); 1.0M 4 planes 12.6 (8: 11.8); 0.3M 2 planes 7.3 (8:
+// 5.6); 31k 2 planes 1.5 (8: 0.7).  Not part of the reference surface.
 extern "C" int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t march_kz) {
   clear_error();
   A3D_ARG(s, "null solver");
@@ -712,11 +714,13 @@ extern "C" int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t marc
   if (march_kz == 0) {
     march_kz = 16;
     if (kernel == KERNEL_TMA) {
-      const long tiles = (long)((s->grid.NX + 31) / 32) * ((s->grid.NY + 7) / 8) * ((s->grid.NZ + 15) / 16);
+      const long columns = (long)((s->grid.NX + 31) / 32) * ((s->grid.NY + 7) / 8);
       int resident = 0;
       A3D_CUDA(cudaSetDevice(s->device));
       A3D_TRY(tma_resident_ctas(&resident));
-      if (tiles < 2L * resident) march_kz = 8;
+      march_kz = 2;
+      for (int kz : {16, 8, 4})
+        if (columns * ((s->grid.NZ + kz - 1) / kz) >= 2L * resident) { march_kz = kz; break; }
     }
   }
   s->kernel = kernel;
