@@ -68,6 +68,7 @@ PROTOS = {
     "a3d_solver_residual_parts": (C.c_int, [_vp, _dp]),
     "a3d_solver_set_neighbors": (C.c_int, [_vp, _vp, _vp]),
     "a3d_solver_set_chunks": (C.c_int, [_vp, C.c_int32]),
+    "a3d_solver_read_dt": (C.c_int, [_vp, C.c_void_p]),
     "a3d_solver_get_kernel": (C.c_int, [_vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
     "a3d_solver_get_chunks": (C.c_int, [_vp, C.POINTER(C.c_int32)]),
     "a3d_solver_sync_neighbors": (C.c_int, [_vp]),

@@ -200,6 +200,12 @@ class CfdGPU:
         _lib.check(_lib.lib().a3d_solver_read(self._h, *(_lib.ptr(out[k]) for k in ("r", "ru", "rv", "rw", "E"))))
         return out
 
+    def read_dt(self):
+        """The `dt` field of CfdGPU.read(): each fluid cell's local time step in the last iteration."""
+        out = np.empty(self.g.N, np.float32)
+        _lib.check(_lib.lib().a3d_solver_read_dt(self._h, _lib.ptr(out)))
+        return out
+
     def read_array(self):
         H = self.read()
         return np.stack([H[k] for k in ("r", "ru", "rv", "rw", "E")]).copy()

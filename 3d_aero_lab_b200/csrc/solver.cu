@@ -48,6 +48,26 @@ __global__ void k_codes(int NX, int NY, int NZ, int NXp, const uint8_t* t, const
   }
 }
 
+// Local time step of every fluid cell from a state (the stage kernels' arithmetic: rsqrt sound
+// speed, reciprocal sizes); 0 for the other cells, as the reference's shader leaves them.
+__global__ void k_local_dt(StageArgs a, const float* __restrict__ Q, float* __restrict__ dt) {
+  const long NXY = (long)a.NX * a.NY, N = NXY * a.NZ;
+  for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < N; q += (long)gridDim.x * blockDim.x) {
+    const int i = (int)(q % a.NX), j = (int)((q / a.NX) % a.NY), k = (int)(q / NXY);
+    const long qp = ((long)k * a.NY + j) * a.NXp + i;
+    float v = 0.f;
+    if ((a.code[qp] & 7) == T_FLUID) {
+      float P[5];
+      cons_to_prim(Q[qp], Q[a.Np + qp], Q[2 * a.Np + qp], Q[3 * a.Np + qp], Q[4 * a.Np + qp], P);
+      const float ph = (a.code[qp] & C_IRR) ? a.phi[q] : 1.f;
+      const float gp = kG * P[4], as = gp * rsqrtf(gp * P[0]);
+      v = a.cfl * fmaxf(ph, 0.25f) /
+          ((fabsf(P[1]) + as) * a.rXd[i] + (fabsf(P[2]) + as) * a.rYd[j] + (fabsf(P[3]) + as) * a.rZd[k]);
+    }
+    dt[q] = v;
+  }
+}
+
 __global__ void k_fill(float* Q, long Np, float f0, float f1, float f2, float f3, float f4) {
   for (long q = blockIdx.x * (long)blockDim.x + threadIdx.x; q < Np; q += (long)gridDim.x * blockDim.x) {
     Q[q] = f0; Q[Np + q] = f1; Q[2 * Np + q] = f2; Q[3 * Np + q] = f3; Q[4 * Np + q] = f4;
@@ -660,6 +680,32 @@ extern "C" int a3d_solver_plane_ptr(a3d_solver* s, int32_t which, int32_t c, int
   const long plane = (long)s->grid.NY * s->NXp;
   *ptr = state_buffer(s, which) + c * s->Np + k * plane;
   *plane_floats = plane;
+  return A3D_OK;
+}
+
+// The `dt` field of CfdGPU.read() (src/air_cfd.js:435): the local time step of each fluid cell
+// in the solver's last iteration, formed from that iteration's base state, which stays in the
+// B buffer after the swap; 0 for the other cells and before the first iteration.  Cell order
+// as a3d_solver_read; synchronises.
+extern "C" int a3d_solver_read_dt(a3d_solver* s, float* dt) {
+  clear_error();
+  A3D_ARG(s && dt, "null pointer");
+  A3D_ARG(s->phase == 0, "between the two stages of an iteration");
+  A3D_CUDA(cudaSetDevice(s->device));
+  float* d = nullptr;
+  A3D_CUDA(cudaMallocAsync(&d, s->N * sizeof(float), s->st));
+  if (s->it == 0) {
+    A3D_CUDA(cudaMemsetAsync(d, 0, s->N * sizeof(float), s->st));
+  } else {
+    StageArgs a;
+    fill_stage_args(s, a, nullptr, nullptr, nullptr, 0.f, 1.f);
+    k_local_dt<<<blocks_for(s->N), 256, 0, s->st>>>(a, s->buf[s->iB], d);
+  }
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(dt, d, s->N * sizeof(float), cudaMemcpyDeviceToHost, s->st);
+  cudaFreeAsync(d, s->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+  if (e != cudaSuccess) { set_error("read_dt: %s", cudaGetErrorString(e)); return A3D_ERR_CUDA; }
   return A3D_OK;
 }
 

@@ -143,6 +143,9 @@ int a3d_solver_iterations(a3d_solver* s, int64_t* it);
 /* read() (src/air_cfd.js:259): copies Q into five caller arrays of N floats
  * (rho, rho*u, rho*v, rho*w, E).  Synchronises.                                        */
 int a3d_solver_read(a3d_solver* s, float* r, float* ru, float* rv, float* rw, float* E);
+/* The dt field of CfdGPU.read() (src/air_cfd.js:435): each fluid cell's local time step in the
+ * last iteration, 0 elsewhere and before the first iteration; N floats in cell order.     */
+int a3d_solver_read_dt(a3d_solver* s, float* dt);
 /* Uploads a state (warm start or checkpoint restore); same layout as read(). */
 int a3d_solver_write(a3d_solver* s, const float* r, const float* ru, const float* rv,
                      const float* rw, const float* E);

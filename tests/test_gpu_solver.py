@@ -102,6 +102,32 @@ def test_pipelined_z_chunks_are_bit_identical(aero, chunks):
     assert a.residual(1) == b.residual(1)
 
 
+def test_read_dt_is_the_last_iterations_local_time_step(aero):
+    """CfdGPU.read().dt (src/air_cfd.js:435): per fluid cell cfl max(phi, 1/4) / sum(|u_d| + a)/h_d
+    from the base state of the last iteration; 0 for other cells and before any iteration."""
+    ac = aero.build_aircraft("fighter")
+    sh = aero.shape_of(ac)
+    g, s = gpu_case(aero, sh, 60000, 3.0, kernel=2)
+    geo = aero.cfd_geom(sh, g, 3.0)
+    assert not np.any(s.read_dt())
+    s.step(24)
+    Q = s.read_array().astype(np.float64)
+    s.step(1)
+    dt = s.read_dt()
+    r = np.maximum(Q[0], 1e-6)
+    u, v, w = Q[1] / r, Q[2] / r, Q[3] / r
+    p = np.maximum(0.4 * (Q[4] - 0.5 * r * (u * u + v * v + w * w)), 1e-7)
+    a = np.sqrt(1.4 * p / r)
+    n = np.arange(g.N)
+    i, j, k = n % g.NX, (n // g.NX) % g.NY, n // (g.NX * g.NY)
+    dx, dy, dz = (np.diff(ax.f).astype(np.float32).astype(np.float64) for ax in (g.X, g.Y, g.Z))
+    ref = 0.7 * np.maximum(geo.phi.astype(np.float64), 0.25) / (
+        (np.abs(u) + a) / dx[i] + (np.abs(v) + a) / dy[j] + (np.abs(w) + a) / dz[k])
+    fluid = geo.t == 0
+    assert np.all(dt[~fluid] == 0)
+    assert float(np.max(np.abs(dt[fluid] - ref[fluid]) / ref[fluid])) < 2e-6
+
+
 @pytest.mark.parametrize("kernel", [1, 2, 3])
 def test_kernels_agree(aero, kernel):
     """The tiled kernels against the per-cell one (same float32 arithmetic, other summation order)."""
