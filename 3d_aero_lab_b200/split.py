@@ -280,10 +280,11 @@ class DistSplit:
             self.it += 1
 
     def _allreduce(self, values, op):
+        # host values (the slab's reductions have synchronised): reduce on the stream that made
+        # the tensor
         import torch
         t = torch.tensor(values, dtype=torch.float64, device=self.device)
-        with self.slab.stream():
-            self.dist.all_reduce(t, op=op, group=self.group)
+        self.dist.all_reduce(t, op=op, group=self.group)
         return t.tolist()
 
     def forces(self, alpha, M, ref, xT):
