@@ -194,3 +194,20 @@ def test_throttle_lowers_the_jet_speed(aircraft):
     ac = aircraft["airliner"]
     u = [prim(Fm.fix_states(ac, 0.0, 0.6, 3.0, thr)[1][2])[1] for thr in (0.6, 0.8, 1.0)]
     assert u[0] < u[1] < u[2]
+
+
+def test_fix_states_match_the_committed_record():
+    """Regression record of fix_states (tests/golden/make_field_golden.py)."""
+    import json
+    import os
+    import sys
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    rec = json.load(open(os.path.join(here, "field_fix_states.json")))
+    sys.path.insert(0, here)
+    import make_field_golden
+    now = make_field_golden.states()
+    assert len(now) == len(rec["cases"]) == 24
+    for a, b in zip(now, rec["cases"]):
+        assert (a["type"], a["h"], a["M"], a["thr"], a["ab"]) == (b["type"], b["h"], b["M"], b["thr"], b["ab"])
+        for u, v in zip(a["fix"], b["fix"]):
+            assert all(math.isclose(x, y, rel_tol=1e-12, abs_tol=1e-15) for x, y in zip(u, v)), a
