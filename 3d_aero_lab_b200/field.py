@@ -95,6 +95,21 @@ def fs_state(h, M):
             "Tt": at["T"] * k, "Pt": at["P"] * math.pow(k, 3.5), "q": 0.5 * at["rho"] * V * V}
 
 
+def cfd_state(fs, W):
+    """Nondimensional primitives (rho, u, v, w, p) of the solver -> dimensional state at the free
+    stream fs (cfdState, src/air_cfd.js:484-490): P, T, rho, V, M, Tt, Pt, Cp, Taw, Vx, Vy, Vz."""
+    T = CG * W[4] / W[0] * fs["T"]
+    a = math.sqrt(1.4 * 287.05 * T)
+    V = math.hypot(W[1], W[2], W[3]) * fs["a"]
+    o = {"P": W[4] * CG * fs["P"], "T": T, "rho": W[0] * fs["rho"], "V": V, "M": V / a}
+    o["Tt"] = T * (1 + 0.2 * o["M"] * o["M"])
+    o["Pt"] = o["P"] * math.pow(1 + 0.2 * o["M"] * o["M"], 3.5)
+    o["Cp"] = (o["P"] - fs["P"]) / fs["q"] if fs["q"] > 1 else 0
+    o["Taw"] = T * (1 + 0.89 * 0.2 * o["M"] * o["M"])
+    o["Vx"], o["Vy"], o["Vz"] = W[1] * fs["a"], W[2] * fs["a"], W[3] * fs["a"]
+    return o
+
+
 # ---------------------------------------------------------------------------
 # engine deck  (src/perf.js:7-47)
 # ---------------------------------------------------------------------------

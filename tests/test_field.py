@@ -211,3 +211,15 @@ def test_fix_states_match_the_committed_record():
         assert (a["type"], a["h"], a["M"], a["thr"], a["ab"]) == (b["type"], b["h"], b["M"], b["thr"], b["ab"])
         for u, v in zip(a["fix"], b["fix"]):
             assert all(math.isclose(x, y, rel_tol=1e-12, abs_tol=1e-15) for x, y in zip(u, v)), a
+
+
+def test_cfd_state_of_the_free_stream_is_the_free_stream():
+    """cfdState (src/air_cfd.js:484-490) of the solver's free stream gives back the atmosphere."""
+    for h, M in ((0.0, 0.6), (11000.0, 0.78)):
+        fs = Fm.fs_state(h, M)
+        F = Fm.free_state(M, 0.0)
+        W = [F[0], F[1] / F[0], F[2] / F[0], F[3] / F[0], (1.4 - 1) * (F[4] - 0.5 * F[1] ** 2 / F[0])]
+        o = Fm.cfd_state(fs, W)
+        assert math.isclose(o["P"], fs["P"], rel_tol=1e-12) and math.isclose(o["T"], fs["T"], rel_tol=1e-12)
+        assert math.isclose(o["rho"], fs["rho"], rel_tol=1e-12) and math.isclose(o["M"], M, rel_tol=1e-12)
+        assert abs(o["Cp"]) < 1e-12 and math.isclose(o["Vx"], fs["V"], rel_tol=1e-12)
