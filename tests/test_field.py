@@ -223,3 +223,19 @@ def test_cfd_state_of_the_free_stream_is_the_free_stream():
         assert math.isclose(o["P"], fs["P"], rel_tol=1e-12) and math.isclose(o["T"], fs["T"], rel_tol=1e-12)
         assert math.isclose(o["rho"], fs["rho"], rel_tol=1e-12) and math.isclose(o["M"], M, rel_tol=1e-12)
         assert abs(o["Cp"]) < 1e-12 and math.isclose(o["Vx"], fs["V"], rel_tol=1e-12)
+
+
+def test_app_convergence_rule():
+    """CFD3.readback's test (src/air_cfd.js:575): res/res0 < 2e-3 and the last four C_L within
+    2e-3, with more than six readbacks."""
+    ctl = importlib.import_module("3d_aero_lab_b200.controller")
+    h = [{"CL": 0.3}] * 6
+    assert not ctl.converged(h, 1e-6, 1.0)                       # six readbacks are not enough
+    h = h + [{"CL": 0.3}]
+    assert ctl.converged(h, 1e-3, 1.0)
+    assert not ctl.converged(h, 3e-3, 1.0)                       # residual not low enough
+    assert not ctl.converged(h, 1e-3, None)                      # no first residual yet
+    h2 = h[:-1] + [{"CL": 0.3021}]
+    assert not ctl.converged(h2, 1e-3, 1.0)                      # C_L still moving
+    h3 = [{"CL": 0.5}] * 3 + [{"CL": 0.3}, {"CL": 0.301}, {"CL": 0.3005}, {"CL": 0.3015}]
+    assert ctl.converged(h3, 1e-3, 1.0)                          # only the last four count

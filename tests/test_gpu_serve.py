@@ -70,3 +70,20 @@ def test_grid_sequencing_matches_cold_solves(aero):
         for k in ("CL", "CD"):
             assert abs(seq[k] - cold[k]) < 1e-3, (k, seq[k], cold[k])
     assert sum(s["iterations"] for s in runs[8]) < sum(c["iterations"] for c in runs[0])
+
+
+def test_app_controller_loop(aero):
+    """The app's loop (CFD3.tick/readback) on a small case: readbacks every 100 iterations until
+    its convergence rule holds or 3000 iterations have run."""
+    ctl = importlib.import_module("3d_aero_lab_b200.controller")
+    case = aero.Case(aircraft_type="fighter", cells=30000, M=0.6, alpha=3.0, delta=3.0)
+    c = ctl.Controller(case, check_every=100)
+    rec = c.run(max_iters=3000)
+    assert rec is not None and len(c.hist) == case.solver.it // 100
+    assert c.res0 and c.res0 > 0 and all(h["res"] is None or h["res"] > 0 for h in c.hist)
+    assert 0 < rec["Mmax"] < 3 and rec["CDi"] >= 0
+    if c.conv:
+        assert c.res / c.res0 < 2e-3
+    f = case.forces()
+    assert f["CL"] == rec["CL"]
+    case.solver.dispose()
