@@ -71,8 +71,15 @@ def _shape(x):
     return x if isinstance(x, a3d_shape) else shape_of(x)
 
 
+# the app's grid levels (CFD_GRIDS, src/air_cfd.js:10)
+CFD_GRIDS = {"coarse": 150e3, "medium": 380e3, "fine": 820e3}
+
+
 def cfd_grid(ac, cells):
-    """Stretched half-domain grid with about `cells` cells (cfdGrid, src/air_cfd.js:21-44)."""
+    """Stretched half-domain grid with about `cells` cells, or a level name of CFD_GRIDS
+    (cfdGrid, src/air_cfd.js:21-44)."""
+    if isinstance(cells, str):
+        cells = CFD_GRIDS[cells]
     sh = _shape(ac)
     L = _lib.lib()
     xf, yf, zf = (np.zeros(MAX_FACES) for _ in range(3))

@@ -101,3 +101,11 @@ def test_slab_and_chunk_entry_points_check_their_arguments():
     for rc in calls:
         assert rc != 0
         assert lib.a3d_last_error()
+
+
+def test_grid_levels_are_the_apps(aero):
+    """cfdGrid(ac, level) with the app's CFD_GRIDS (src/air_cfd.js:10)."""
+    sh = aero.shape_of(aero.build_aircraft("fighter"))
+    for level, cells in (("coarse", 150e3), ("medium", 380e3), ("fine", 820e3)):
+        a, b = aero.cfd_grid(sh, level), aero.cfd_grid(sh, cells)
+        assert (a.NX, a.NY, a.NZ) == (b.NX, b.NY, b.NZ) and abs(a.N / cells - 1) < 0.06
