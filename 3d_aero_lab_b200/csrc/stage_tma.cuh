@@ -173,11 +173,6 @@ __device__ __forceinline__ bool stage_tile(TmaSmem& S, const CUtensorMap* tmQ, c
   for (int k = k0; k < k1; k++) {
     const long q = ((long)k * a.NY + j) * a.NX + i;    // geometry (reference) index
     const long qp = ((long)k * a.NY + j) * a.NXp + i;  // padded state index
-    float bq[5];
-    if (STAGE2 && in_dom) {
-#pragma unroll
-      for (int c = 0; c < 5; c++) bq[c] = __ldg(Bp + c * Np + qp);
-    }
     // ---- plane k+2 into the column window; plane k to shared memory ----
     const int sk = slot_of(k, k0), sk2 = slot_of(k + 2, k0);
     ok = mbar_wait(&S.bar[sk2], parity_of(k + 2, k0));
@@ -239,6 +234,11 @@ __device__ __forceinline__ bool stage_tile(TmaSmem& S, const CUtensorMap* tmQ, c
         for (int v = 0; v < 5; v++) S.Fx[v][row][TX] = G[v];
         S.Ax[row][TX] = A;
       }
+    }
+    float bq[5];
+    if (STAGE2 && in_dom) {
+#pragma unroll
+      for (int c = 0; c < 5; c++) bq[c] = __ldg(Bp + c * Np + qp);
     }
     float Gn[5], An = 1.f;
     float Ln[5];
