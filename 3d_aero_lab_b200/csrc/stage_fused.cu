@@ -1,4 +1,4 @@
-// stage_fused.cu - single-case launch of the fused RK-stage tile (KERNEL_FUSED, the default).
+// stage_fused.cu - single-case launch of the fused RK-stage tile (KERNEL_FUSED, stage kernel 3).
 // One CTA per tile: grid (ceil(NX/32), ceil(NY/8), ceil(NZ/kz)).  See stage_fused.cuh.
 #include "stage_fused.cuh"
 

@@ -1,4 +1,4 @@
-// stage_fused.cuh - the RK-stage tile with per-cell face states (KERNEL_FUSED, the default).
+// stage_fused.cuh - the RK-stage tile with per-cell face states (KERNEL_FUSED, stage kernel 3).
 //
 // Tiling and plane ring as stage_tma.cu (32 x 8 columns per CTA, z march, TMA ring of 4
 // planes).  What changes is how a face is evaluated:
