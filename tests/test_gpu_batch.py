@@ -112,3 +112,24 @@ def test_tuner_restores_state_and_picks_a_schedule(aero, kernel):
     b.step(2)
     b.sync()
     b.dispose()
+
+
+def test_stream_mode_captures_chunked_steps(aero):
+    """Mode 1 captures each case's own step; a case stepped as pipelined z chunks (its own
+    streams and events) is captured into the batch graph and stays bit-identical."""
+    cases = [("fighter", 200000, 0.6, 3.0, 3.0), ("airliner", 150000, 0.78, 2.5, 0.0)]
+    alone = [make(aero, 2, *c) for c in cases]
+    batched = [make(aero, 2, *c) for c in cases]
+    for k, c in enumerate(alone + batched):
+        c.solver.set_kernel(2, 4)
+        c.solver.set_chunks(3 + k % 2)
+    assert all(c.solver.chunks() > 1 for c in alone + batched)
+    for c in alone:
+        c.solver.step(9)
+    b = aero.Batch([c.solver for c in batched])
+    b.set_mode(1)
+    b.step(9)
+    b.sync()
+    for a, c in zip(alone, batched):
+        assert np.array_equal(c.solver.read_array(), a.solver.read_array())
+    b.dispose()
