@@ -115,8 +115,9 @@ def test_tuner_restores_state_and_picks_a_schedule(aero, kernel):
 
 
 def test_stream_mode_captures_chunked_steps(aero):
-    """Mode 1 captures each case's own step; a case stepped as pipelined z chunks (its own
-    streams and events) is captured into the batch graph and stays bit-identical."""
+    """Cases set to pipelined z chunks (their own streams and events): the batch graph runs
+    their whole-case stage launches and the odd iteration runs as their own chunked step, and
+    the result stays bit-identical to the cases stepped alone (chunked throughout)."""
     cases = [("fighter", 200000, 0.6, 3.0, 3.0), ("airliner", 150000, 0.78, 2.5, 0.0)]
     alone = [make(aero, 2, *c) for c in cases]
     batched = [make(aero, 2, *c) for c in cases]
