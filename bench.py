@@ -179,17 +179,33 @@ def barrier(ws):
         dist.barrier()
 
 
-def cpu_baseline(aero, sh, cells, iters, threads, M, alpha, delta):
-    """The oracle (C++ CfdCPU restatement, f32 storage / f64 arithmetic) on a bounded sample."""
+def workload_config(args, g):
+    """The `config` keys both arms share: the plain solve they time, named by its sizes."""
+    return {"workload": f"{args.aircraft} plain solve, {g.NX}x{g.NY}x{g.NZ} = {g.N} cells, "
+                        f"M{args.mach} a{args.alpha} d{args.delta}, {args.iters} SSP-RK2 iterations per step",
+            "cells": g.N, "dims": [g.NX, g.NY, g.NZ], "iterations_per_step": args.iters,
+            "fixed_states": args.fix if args.fix == "free" else f"cycle at {args.altitude:g} m"}
+
+
+def oracle_solver(aero, args, ac, threads):
+    """The oracle (C++ CfdCPU restatement, f32 storage / f64 arithmetic) set up on the bench's
+    case: same grid, geometry, free stream and fixed states as the GPU arm."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref
-    g = ref.grid(sh, cells)
-    geo = ref.geom(sh, g, delta)
+    sh = aero.shape_of(ac)
+    g = ref.grid(sh, args.cells)
+    geo = ref.geom(sh, g, args.delta)
     s = ref.CfdCPU(g, geo, threads=threads)
-    F = aero.cfd.freestream(M, alpha)
+    F = aero.cfd.freestream(args.mach, args.alpha)
     s.setFree(F)
-    s.setFix([F, F, F])
+    s.setFix(aero.fix_states(ac, args.altitude, args.mach, args.alpha)[1] if args.fix == "cycle" else [F, F, F])
     s.reset()
+    return s, g
+
+
+def cpu_baseline(aero, args, ac, iters, threads):
+    """The oracle on a bounded sample of the bench's case: iters timed iterations."""
+    s, g = oracle_solver(aero, args, ac, threads)
     s.step(1)  # untimed warm-up iteration
     t0 = time.perf_counter()
     s.step(iters)
@@ -357,16 +373,8 @@ def run_reference(args, ws, rank):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref
     threads = ref.max_threads()
-    ac = aero.build_aircraft(WORKLOAD["aircraft"])
-    sh = aero.shape_of(ac)
-    g = ref.grid(sh, args.cells)
-    geo = ref.geom(sh, g, WORKLOAD["delta"])
-    s = ref.CfdCPU(g, geo, threads=threads)
-    F = aero.cfd.freestream(WORKLOAD["M"], WORKLOAD["alpha"])
-    s.setFree(F)
-    s.setFix(aero.fix_states(ac, args.altitude, WORKLOAD["M"], WORKLOAD["alpha"])[1] if args.fix == "cycle"
-             else [F, F, F])
-    s.reset()
+    ac = aero.build_aircraft(args.aircraft)
+    s, g = oracle_solver(aero, args, ac, threads)
     per_step = max(1, args.cpu_sample_iters)
     for _ in range(args.warmup):
         s.step(1)
@@ -375,13 +383,15 @@ def run_reference(args, ws, rank):
         s.step(per_step)
     dt = time.perf_counter() - t0
     v = g.N * per_step * args.steps / dt
-    sample = f"{per_step} iterations per step of the {g.NX}x{g.NY}x{g.NZ} fighter grid"
+    sample = (f"{per_step} iterations per step of the {g.NX}x{g.NY}x{g.NZ} {args.aircraft} case, "
+              f"{threads} threads (C++ restatement of CfdCPU; the JavaScript original cannot run here)")
+    config = workload_config(args, g)
+    config["parallelism"] = f"host CPU, {threads} threads"
     out = {"metric": "cell-updates/s", "value": v, "unit": "cell-updates/s", "n_gpus": args.gpus,
            "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
            "impl": "reference",
-           "config": {"workload": "fighter plain solve, CPU reference algorithm (C++ CfdCPU restatement)",
-                      "cells": g.N, "dims": [g.NX, g.NY, g.NZ]},
+           "config": config,
            "cpu_baseline": {"value": v, "unit": "cell-updates/s", "cores": threads, "kind": "port", "sample": sample},
            "e2e": {"value": v, "unit": "cell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)
@@ -399,7 +409,6 @@ def main():
     torch.cuda.set_device(local)
     alpha = args.alpha + 0.25 * rank  # independent case per rank
     ac = aero.build_aircraft(args.aircraft)
-    sh = aero.shape_of(ac)
     case = aero.Case(ac=ac, cells=args.cells, M=args.mach, alpha=alpha, delta=args.delta, device=local,
                      fixed=args.fix, h=args.altitude)
     s = case.solver
@@ -486,17 +495,14 @@ def main():
     if rank == 0:
         cpu = None
         if not args.no_cpu_baseline and ws == 1:
-            v, n_cpu = cpu_baseline(aero, sh, args.cells, args.cpu_sample_iters, 1, args.mach, args.alpha, args.delta)
+            v, n_cpu = cpu_baseline(aero, args, ac, args.cpu_sample_iters, 1)
             cpu = {"value": v, "unit": "cell-updates/s", "cores": 1, "kind": "port",
                    "sample": f"{args.cpu_sample_iters} iterations of the same {g.NX}x{g.NY}x{g.NZ} grid, 1 thread "
                              "(C++ restatement of CfdCPU; the JavaScript original cannot run here)"}
         out = {"metric": "cell-updates/s", "value": value, "unit": "cell-updates/s", "n_gpus": ws,
                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
                "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-               "config": {"workload": f"{args.aircraft} plain solve, {g.NX}x{g.NY}x{g.NZ} = {N} cells, "
-                                      f"M{args.mach} a{args.alpha} d{args.delta}, {iters} SSP-RK2 iterations per step",
-                          "cells": N, "dims": [g.NX, g.NY, g.NZ], "iterations_per_step": iters,
-                          "fixed_states": args.fix if args.fix == "free" else f"cycle at {args.altitude:g} m",
+               "config": {**workload_config(args, g),
                           "kernel": {0: "cell", 1: "march", 2: "tma", 3: "fused"}[args.kernel], "march_kz": kz_used,
                           "z_chunks": chunks,
                           "l2": "inputs larger than L2 (three 5-component float32 states of %.0f MB each)"
