@@ -83,6 +83,28 @@ def test_engine_field_fixed_states_match_oracle(aero, ref, typ, cells, h, M, alp
     assert sig4(fg["CL"]) == sig4(fo["CL"]) and sig4(fg["CD"]) == sig4(fo["CD"])
 
 
+@pytest.mark.parametrize("typ,cells,M,alpha,delta", [("interceptor", 60000, 0.85, 8.0, -5.0),
+                                                     ("airliner", 40000, 0.3, -2.0, 5.0)])
+def test_batch_distribution_corners_match_oracle(aero, ref, typ, cells, M, alpha, delta):
+    """Corners of the batched/served case distribution (M 0.3-0.85, alpha -2..8, delta -5..5) on
+    the other two aircraft: the default kernel against the oracle, same tolerances as the README
+    case."""
+    ac, sh, og, ogeo, o = oracle_case(aero, ref, typ, cells, delta, M=M, alpha=alpha)
+    g, s = gpu_case(aero, sh, cells, delta, M=M, alpha=alpha, kernel=2)
+    o.step(200)
+    s.step(200)
+    Qo, Qg = o.read(), s.read_array()
+    assert np.all(np.isfinite(Qg))
+    errs = [rel_max_diff(Qg[c], Qo[c]) for c in range(5)]
+    assert all(e <= t for e, t in zip(errs, TOL_GPUCMP)), errs
+    for c in (0, 4):
+        assert float(np.max(np.abs(Qg[c] - Qo[c]) / np.abs(Qo[c]))) <= TOL_CELL, c
+    r = ac.ref
+    fg = s.forces(alpha, M, r["S"], r["xcg"], 0.0, r["c"])
+    fo = o.forces(alpha, M, r["S"], r["xcg"], 0.0, r["c"])
+    assert sig4(fg["CL"]) == sig4(fo["CL"]) and sig4(fg["CD"]) == sig4(fo["CD"])
+
+
 @pytest.mark.parametrize("chunks", [0, 2, 3, 4])
 def test_pipelined_z_chunks_are_bit_identical(aero, chunks):
     """The TMA kernel stepped as z chunks on their own streams, each waiting only for its
