@@ -746,11 +746,12 @@ extern "C" int a3d_solver_write(a3d_solver* s, const float* r, const float* ru, 
 }
 
 // Selects the stage kernel (0: per-cell, 1: z-march, 2: TMA, 3: fused) and the z planes per
-// CTA of the tiled kernels.  march_kz = 0 picks it for the TMA tile: the longest run of 16, 8 or
-// 4 planes that still launches two waves of CTAs (column tiles x z runs >= 2 x resident CTAs),
-// else 2.  Shorter runs cost more ring prologue per plane but keep the SMs busy and the z chunks
-// of a3d_solver_step overlapping.  Measured (G cell-updates/s, fighter): 4.1M cells 16 planes
-// 15.1; 2.0M 8 planes 13.5 (16: 12.2); 1.0M 4 planes 12.6 (8: 11.8); 0.3M 2 planes 7.3 (8:
+// CTA of the tiled kernels.  march_kz = 0 picks it for the TMA tile: 32 planes where that still
+// launches four waves of CTAs (column tiles x z runs >= 4 x resident CTAs), else the longest run
+// of 16, 8 or 4 planes that launches two waves, else 2.  Shorter runs cost more ring prologue
+// per plane but keep the SMs busy and the z chunks of a3d_solver_step overlapping.  Measured
+// (G cell-updates/s, fighter): 15.8M cells 32 planes 16.0 (16: 15.7); 4.1M 16 planes 15.1 (32:
+// 13.8); 2.0M 8 planes 13.5 (16: 12.2); 1.0M 4 planes 12.6 (8: 11.8); 0.3M 2 planes 7.3 (8:
 // 5.6); 31k 2 planes 1.5 (8: 0.7).  Not part of the reference surface.
 extern "C" int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t march_kz) {
   clear_error();
@@ -764,9 +765,12 @@ extern "C" int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t marc
       int resident = 0;
       A3D_CUDA(cudaSetDevice(s->device));
       A3D_TRY(tma_resident_ctas(&resident));
+      auto ctas = [&](int kz) { return columns * ((s->grid.NZ + kz - 1) / kz); };
       march_kz = 2;
-      for (int kz : {16, 8, 4})
-        if (columns * ((s->grid.NZ + kz - 1) / kz) >= 2L * resident) { march_kz = kz; break; }
+      if (ctas(32) >= 4L * resident) march_kz = 32;
+      else
+        for (int kz : {16, 8, 4})
+          if (ctas(kz) >= 2L * resident) { march_kz = kz; break; }
     }
   }
   s->kernel = kernel;
