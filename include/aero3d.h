@@ -183,8 +183,9 @@ int a3d_solver_interp_state(a3d_solver* fine, const a3d_solver* coarse);
  * kernel 2 (default): the same fed by a TMA plane ring, three CTAs per SM;
  * kernel 3: TMA ring, face states formed once per cell, paired f32x2 faces; results do
  *           not depend on the tiling.
- * march_kz = z planes per thread block; 0 (the default) picks for the TMA tile the longest of
- * 16, 8 or 4 planes that still launches two waves of CTAs, else 2.                    */
+ * march_kz = z planes per thread block; 0 (the default) picks for the TMA tile 32 planes if
+ * that still launches four waves of CTAs, else the longest of 16, 8 or 4 planes that
+ * launches two waves, else 2.                                                            */
 int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t march_kz);
 int a3d_solver_get_kernel(a3d_solver* s, int32_t* kernel, int32_t* march_kz);
 /* Kernel 2 steps the case as up to 4 z chunks of whole z runs on their own streams, each
