@@ -239,3 +239,64 @@ def test_app_convergence_rule():
     assert not ctl.converged(h2, 1e-3, 1.0)                      # C_L still moving
     h3 = [{"CL": 0.5}] * 3 + [{"CL": 0.3}, {"CL": 0.301}, {"CL": 0.3005}, {"CL": 0.3015}]
     assert ctl.converged(h3, 1e-3, 1.0)                          # only the last four count
+
+
+class _FakeSolver:
+    """Stands in for CfdGPU in the controller loop: the residual decays geometrically with the
+    iterations and C_L settles towards 0.3."""
+
+    def __init__(self, decay):
+        self.it = 0
+        self.decay = decay
+        self.snap = False
+
+    def step(self, n):
+        self.it += n
+
+    def residual(self, stride=3):
+        if not self.snap:  # the first call only snapshots, as the device residual does
+            self.snap = True
+            return None
+        return 1e-2 * self.decay ** self.it
+
+    def mach_max(self, stride=2):
+        return 0.9
+
+
+class _FakeCase:
+    def __init__(self, decay):
+        self.solver = _FakeSolver(decay)
+
+    def forces(self):
+        return {"CL": 0.3 + 0.2 * math.exp(-self.solver.it / 300.0), "CD": 0.04, "Cm": -0.1}
+
+    def trefftz(self):
+        return 0.01
+
+
+def test_controller_loop_stops_by_the_app_rule():
+    """Controller.run on a case whose residual falls 100x per 1000 iterations: it stops at the
+    first readback where res/res0 < 2e-3 and the last four C_L lie within 2e-3."""
+    ctl = importlib.import_module("3d_aero_lab_b200.controller")
+    c = ctl.Controller(_FakeCase(0.01 ** (1 / 1000)), check_every=200)
+    rec = c.run()
+    assert c.conv and rec["it"] == c.it and c.it % 200 == 0
+    assert c.res / c.res0 < ctl.Controller.RES_DROP
+    cl = [h["CL"] for h in c.hist[-4:]]
+    assert max(cl) - min(cl) < ctl.Controller.CL_TOL
+    # the readback before did not yet meet the rule
+    assert not ctl.converged(c.hist[:-1], c.hist[-2]["res"], c.res0)
+    assert c.res0 == c.hist[0]["res"] and len(c.hist) == c.it // 200
+
+
+def test_controller_loop_stops_at_the_iteration_cap():
+    """A case whose residual never drops stops on the first readback past 30,000 iterations
+    (the app's `it > 30000`)."""
+    ctl = importlib.import_module("3d_aero_lab_b200.controller")
+    c = ctl.Controller(_FakeCase(1.0), check_every=1000)
+    c.run()
+    assert c.conv and c.it == ctl.Controller.MAX_ITERS + 1
+    assert not ctl.converged(c.hist, c.res, c.res0)  # the cap, not the residual rule
+    c2 = ctl.Controller(_FakeCase(1.0), check_every=1000)
+    c2.run(max_iters=2500)  # a bounded run stops at its own limit, not converged
+    assert not c2.conv and c2.it == 2500
