@@ -124,3 +124,38 @@ def test_grid_levels_are_the_apps(aero):
     for level, cells in (("coarse", 150e3), ("medium", 380e3), ("fine", 820e3)):
         a, b = aero.cfd_grid(sh, level), aero.cfd_grid(sh, cells)
         assert (a.NX, a.NY, a.NZ) == (b.NX, b.NY, b.NZ) and abs(a.N / cells - 1) < 0.06
+
+
+def test_every_entry_point_refuses_null_arguments():
+    """Every declared function called with null pointers and zero sizes returns A3D_ERR_ARG with
+    a message, on any machine (the argument checks come before any device work); the destroy
+    functions accept a null handle like free()."""
+    from importlib import import_module
+    L = import_module("3d_aero_lab_b200._lib")
+    L.lib()
+    raw = C.CDLL(L.LIB_PATH)  # separate function objects: pointer arguments as plain void*
+    raw.a3d_last_error.restype = C.c_char_p
+    destroy = {"a3d_solver_destroy", "a3d_batch_destroy", "a3d_server_destroy"}
+    checked = 0
+    for name in declared_functions():
+        if name in ("a3d_last_error", "a3d_abi_version"):
+            continue
+        _, args = L.PROTOS[name]
+        types, vals = [], []
+        for t in args:
+            if t is C.c_double:
+                types.append(t); vals.append(0.0)
+            elif t in (C.c_int, C.c_int32, C.c_int64):
+                types.append(t); vals.append(0)
+            else:
+                types.append(C.c_void_p); vals.append(None)
+        f = raw[name]
+        f.argtypes, f.restype = types, C.c_int
+        rc = f(*vals)
+        if name in destroy:
+            assert rc == 0, name
+        else:
+            assert rc == 1, (name, rc)
+            assert raw.a3d_last_error().startswith(b"bad argument"), name
+        checked += 1
+    assert checked == len(declared_functions()) - 2
