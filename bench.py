@@ -54,6 +54,8 @@ def measured_traffic(kernel, cells):
         if len(f) == 3 and f[0] == "traffic" and f[1] == kernel:
             return float(f[2]) * cells
     return None
+
+
 WORKLOAD = {"aircraft": "fighter", "cells": 4.0e6, "M": 0.6, "alpha": 3.0, "delta": 3.0, "iters": 2000}
 
 
