@@ -17,6 +17,12 @@ constexpr int QBX = 40;  // state box width: x from i0-4 (16-byte aligned start)
 constexpr int CBX = 64;  // code box width: x from i0-16
 constexpr int NSLOT = 4;
 constexpr uint32_t kQBytes = 5 * HY * QBX * 4, kCBytes = HY * CBX;
+// A tiled TMA copy needs its innermost coordinate times the element size to be a multiple of
+// 16 bytes.  Tiles start at i0 = bx * TX, so the state box at x = i0 - 4 (float) and the code
+// box at x = i0 - 16 (u8) are aligned whenever TX is a multiple of 16.
+static_assert(TX % 16 == 0, "TMA box x origins must stay 16-byte aligned");
+static_assert((QBX * 4) % 16 == 0 && CBX % 16 == 0, "TMA box rows must be whole 16-byte units");
+static_assert(kQBytes % 16 == 0 && kCBytes % 16 == 0, "TMA transaction sizes must be 16-byte multiples");
 
 struct __align__(128) Slot {
   float Q[5][HY][QBX];  // conservative state of one plane
