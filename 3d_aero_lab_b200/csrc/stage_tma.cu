@@ -51,6 +51,10 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 
 }  // namespace
 
+// Three CTAs per SM need three tiles' shared memory (plus the 1 KB the hardware reserves per
+// CTA) within the SM's 228 KB.
+static_assert(3 * (sizeof(TmaSmem) + 128 + 1024) <= 228 * 1024, "the TMA tile no longer fits three CTAs per SM");
+
 size_t tma_smem_bytes() { return sizeof(TmaSmem) + 128; }
 
 int tma_resident_ctas(int* n) {
