@@ -65,6 +65,54 @@ def test_uniform_freestream_is_fixed_point(ref):
         assert np.all(Q[c] == np.float32(F[c]))
 
 
+def test_fluxes_telescope_on_an_all_fluid_box(ref):
+    """Conservation: on an all-fluid box whose boundary ring stays at the free stream, one
+    SSP-RK2 iteration of the FP64 run changes each cell by dt_i (R_i(Q) + R_i(S1)) / 2, and the
+    residuals sum to zero over the box because every interior face flux enters its two cells
+    with opposite signs (src/air_cfd.js:223-225).  So sum_i vol_i (Q'_i - Q_i) / dt_i vanishes to
+    rounding, with dt_i the stage-1 local time step (src/air_cfd.js:243)."""
+    NX, NY, NZ = 24, 22, 24
+    N = NX * NY * NZ
+    xf, yf, zf = np.linspace(0, 12, NX + 1), np.linspace(0, 11, NY + 1), np.linspace(-6, 6, NZ + 1)
+    g = ref.Grid(xf, yf, zf)
+    geo = ref.Geom()
+    geo.t = np.zeros(N, np.uint8)
+    geo.phi = np.ones(N, np.float32)
+    geo.ap = [np.ones(N, np.float32)] * 3 + [np.zeros(N, np.float32)]
+    s = ref.CfdCPU(g, geo, prec=64)
+    F = [1.0, 0.5, 0.0, 0.25, 2.0]
+    s.setFree(F)
+    s.setFix([F, F, F])
+    s.reset()
+    # an uneven random blob in the middle; it spreads 2 cells per stage, far from the boundary
+    rng = np.random.default_rng(3)
+    q = np.arange(N)
+    i, j, k = q % NX, (q // NX) % NY, q // (NX * NY)
+    blob = (abs(i - 12) <= 3) & (abs(j - 12) <= 3) & (abs(k - 12) <= 3)
+    Q = np.array([np.full(N, f) for f in F])
+    Q[0][blob] *= 1 + 0.2 * rng.random(blob.sum())
+    Q[1][blob] += 0.1 * rng.standard_normal(blob.sum())
+    Q[2][blob] += 0.1 * rng.standard_normal(blob.sum())
+    Q[4][blob] *= 1 + 0.3 * rng.random(blob.sum())
+    s.write(Q)
+    Q0 = np.array([np.asarray(s.read()[c], np.float64) for c in range(5)])
+    r = np.maximum(Q0[0], 1e-6)
+    u, v, w = Q0[1] / r, Q0[2] / r, Q0[3] / r
+    p = np.maximum(0.4 * (Q0[4] - 0.5 * r * (u * u + v * v + w * w)), 1e-7)
+    a = np.sqrt(1.4 * p / r)
+    dx, dy, dz = (np.diff(f).astype(np.float32).astype(np.float64) for f in (xf, yf, zf))
+    dt = 0.7 / ((abs(u) + a) / dx[i] + (abs(v) + a) / dy[j] + (abs(w) + a) / dz[k])
+    s.step(1)
+    Q1 = np.array([np.asarray(s.read()[c], np.float64) for c in range(5)])
+    changed = np.any(Q1 != Q0, axis=0)
+    assert changed.sum() > 1000
+    assert i[changed].min() >= 4 and i[changed].max() < NX - 4 and k[changed].min() >= 4  # boundary ring untouched
+    vol = dx[i] * dy[j] * dz[k]
+    for c in range(5):
+        t = vol * (Q1[c] - Q0[c]) / dt
+        assert abs(t.sum()) <= 1e-13 * np.abs(t).sum(), c
+
+
 def test_symmetric_inputs_give_symmetric_fp64_and_fp32(aero, ref):
     """FP32-storage and FP64-storage runs of the same scheme stay close (error vs FP64 is small)."""
     ac, sh, g, geo, s32 = oracle_case(aero, ref, "fighter", 8000, 0.0, prec=32)
