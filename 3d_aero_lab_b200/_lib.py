@@ -70,6 +70,7 @@ PROTOS = {
     "a3d_solver_set_chunks": (C.c_int, [_vp, C.c_int32]),
     "a3d_solver_read_dt": (C.c_int, [_vp, C.c_void_p]),
     "a3d_solver_get_kernel": (C.c_int, [_vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+    "a3d_solver_set_wait_limit": (C.c_int, [_vp, C.c_uint32]),
     "a3d_solver_get_chunks": (C.c_int, [_vp, C.POINTER(C.c_int32)]),
     "a3d_solver_sync_neighbors": (C.c_int, [_vp]),
     "a3d_batch_create": (C.c_int, [C.POINTER(_vp), C.c_int32, C.POINTER(_vp)]),

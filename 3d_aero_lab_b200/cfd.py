@@ -167,8 +167,14 @@ class CfdGPU:
         _lib.check(_lib.lib().a3d_solver_get_kernel(self._h, C.byref(k), C.byref(kz)))
         return k.value, kz.value
 
+    WAIT_LIMIT_DEFAULT = 4194304
+
+    def set_wait_limit(self, limit):
+        """Try_waits a stage kernel spends on one TMA copy before it gives up (0: at once)."""
+        _lib.check(_lib.lib().a3d_solver_set_wait_limit(self._h, int(limit)))
+
     def set_chunks(self, chunks):
-        """Pipelined z chunks of step() (kernel 2): 0 automatic, 1 none, 2..4 chunks."""
+        """Pipelined z chunks of step() (kernels 2 and 4): 0 automatic, 1 none, 2..4 chunks."""
         _lib.check(_lib.lib().a3d_solver_set_chunks(self._h, int(chunks)))
 
     def chunks(self):

@@ -48,6 +48,7 @@ struct Job {
   size_t coarse_bytes = 0;
   double coarse_res0 = -1;
   long coarse_its = 0;
+  bool planned_warm = false;  // admission promised it a cached case of its geometry
 };
 
 struct Cached {
@@ -55,6 +56,7 @@ struct Cached {
   size_t bytes;
   double res0;
   uint64_t last_use;
+  bool reserved;  // promised to an admitted request: not evicted, not promised twice
 };
 
 size_t case_bytes(const int32_t dims[3]) {
@@ -94,12 +96,14 @@ namespace {
 
 double secs(a3d_server* sv, Clock::time_point t) { return std::chrono::duration<double>(t - sv->t0).count(); }
 
-// Evicts least recently used idle cases until `need` more bytes fit the budget.
+// Evicts least recently used idle cases (none promised to an admitted request) until `need`
+// more bytes fit the budget.  Caller holds sv->mu.
 void make_room(a3d_server* sv, size_t need) {
-  while (!sv->cache.empty() && sv->resident + need > (size_t)sv->cfg.hbm_budget_bytes) {
-    auto lru = sv->cache.begin();
+  while (sv->resident + need > (size_t)sv->cfg.hbm_budget_bytes) {
+    auto lru = sv->cache.end();
     for (auto it = sv->cache.begin(); it != sv->cache.end(); ++it)
-      if (it->second.last_use < lru->second.last_use) lru = it;
+      if (!it->second.reserved && (lru == sv->cache.end() || it->second.last_use < lru->second.last_use)) lru = it;
+    if (lru == sv->cache.end()) return;
     sv->resident -= lru->second.bytes;
     a3d_solver_destroy(lru->second.s);
     sv->cache.erase(lru);
@@ -126,12 +130,19 @@ int start_coarse(a3d_server* sv, Job& j) {
   if (rc != A3D_OK) return rc;
   if (dims[0] < 2 || dims[1] < 2 || dims[2] < 2) return A3D_OK;  // nothing to interpolate from: no sequencing
   const size_t bytes = case_bytes(dims);
-  make_room(sv, bytes);
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    make_room(sv, bytes);
+    sv->resident += bytes;
+  }
   rc = a3d_solver_create_shape(&r.shape, dims, xf.data(), yf.data(), zf.data(), h, r.delta_deg, sv->cfg.device,
                                &j.coarse);
-  if (rc != A3D_OK) return rc;
+  if (rc != A3D_OK) {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->resident -= bytes;
+    return rc;
+  }
   configure_case(sv, j.coarse);
-  sv->resident += bytes;
   j.coarse_bytes = bytes;
   a3d_solver_set_free(j.coarse, r.F);
   a3d_solver_set_fix(j.coarse, r.fix);
@@ -140,17 +151,23 @@ int start_coarse(a3d_server* sv, Job& j) {
   return a3d_solver_residual(j.coarse, 1, &dummy);  // snapshot
 }
 
+// Frees the coarse case of a sequenced request.  Called without sv->mu: it takes the lock only
+// to update the resident bytes.
 void drop_coarse(a3d_server* sv, Job& j) {
   if (!j.coarse) return;
   a3d_solver_destroy(j.coarse);
-  sv->resident -= j.coarse_bytes;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    sv->resident -= j.coarse_bytes;
+  }
   j.coarse = nullptr;
   j.coarse_bytes = 0;
 }
 
 // Coarse case done: the requested case measures its free-stream res0 over one chunk (on the
 // batch's tile, so the value is the one a cold batched run gets), then starts from the
-// coarse state.  The probe chunk counts towards the case's iterations.
+// coarse state.  The probe chunk counts towards the case's iterations.  Runs on the scheduler
+// thread without sv->mu, so that submit, poll and stats are not held up by its GPU work.
 int switch_to_target(a3d_server* sv, Job& j) {
   j.coarse_its = j.coarse->it;
   const int chunk = sv->cfg.chunk_iters;
@@ -166,28 +183,46 @@ int switch_to_target(a3d_server* sv, Job& j) {
   return rc;
 }
 
+// Starts an admitted request: takes the cached case admission promised it (warm start) or
+// builds a new one.  Called without sv->mu; the lock covers only the cache and the resident
+// bytes, the geometry build runs outside it.
 int start_case(a3d_server* sv, Job& j) {
   const a3d_request& r = j.req;
-  std::vector<double> xf(16384), yf(16384), zf(16384);
-  int32_t dims[3];
-  double h, core[5];
-  int rc = a3d_grid_build(&r.shape, r.cells, 16384, xf.data(), yf.data(), zf.data(), dims, &h, core);
-  if (rc != A3D_OK) return rc;
-  j.bytes = case_bytes(dims);
-  auto hit = sv->cfg.warm_start ? sv->cache.find(r.geometry_key) : sv->cache.end();
-  if (hit != sv->cache.end()) {  // warm start: resident geometry and converged state
-    j.s = hit->second.s;
-    j.res0 = hit->second.res0;
-    sv->cache.erase(hit);  // its bytes stay counted in `resident`
-    j.res.warm = 1;
-    sv->warm_starts++;
-  } else {
-    make_room(sv, j.bytes);
+  if (j.planned_warm) {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    auto range = sv->cache.equal_range(r.geometry_key);
+    for (auto it = range.first; it != range.second; ++it)
+      if (it->second.reserved) {  // warm start: resident geometry and converged state
+        j.s = it->second.s;
+        j.res0 = it->second.res0;
+        j.bytes = it->second.bytes;  // the cached case's bytes stay counted in `resident`
+        sv->cache.erase(it);
+        j.res.warm = 1;
+        sv->warm_starts++;
+        break;
+      }
+  }
+  if (!j.res.warm) {
+    std::vector<double> xf(16384), yf(16384), zf(16384);
+    int32_t dims[3];
+    double h, core[5];
+    int rc = a3d_grid_build(&r.shape, r.cells, 16384, xf.data(), yf.data(), zf.data(), dims, &h, core);
+    if (rc != A3D_OK) return rc;
+    {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      j.bytes = case_bytes(dims);
+      make_room(sv, j.bytes);
+      sv->resident += j.bytes;
+    }
     rc = a3d_solver_create_shape(&r.shape, dims, xf.data(), yf.data(), zf.data(), h, r.delta_deg, sv->cfg.device,
                                  &j.s);
-    if (rc != A3D_OK) return rc;
+    if (rc != A3D_OK) {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      sv->resident -= j.bytes;
+      j.s = nullptr;
+      return rc;
+    }
     configure_case(sv, j.s);
-    sv->resident += j.bytes;
   }
   a3d_solver_set_free(j.s, r.F);
   a3d_solver_set_fix(j.s, r.fix);
@@ -199,6 +234,9 @@ int start_case(a3d_server* sv, Job& j) {
   return A3D_OK;
 }
 
+// Completes a request: its FP64 forces and Trefftz drag (GPU work, without sv->mu), then under
+// the lock the result, the cache and the resident bytes; a case that is not kept is freed
+// after the lock is released.
 void finish_case(a3d_server* sv, Job& j, int status) {
   a3d_result& o = j.res;
   o.status = status;
@@ -218,17 +256,22 @@ void finish_case(a3d_server* sv, Job& j, int status) {
   o.t_submit = secs(sv, j.t_submit);
   o.t_admit = secs(sv, j.t_admit);
   o.t_done = secs(sv, j.t_done);
-  if (j.s) {
-    if (status == A3D_OK && sv->cfg.warm_start) {
-      sv->cache.insert({j.req.geometry_key, Cached{j.s, j.bytes, j.res0, ++sv->tick}});
-    } else {
-      sv->resident -= j.bytes;
-      a3d_solver_destroy(j.s);
+  a3d_solver* discard = nullptr;
+  {
+    std::lock_guard<std::mutex> lk(sv->mu);
+    if (j.s) {
+      if (status == A3D_OK && sv->cfg.warm_start) {
+        sv->cache.insert({j.req.geometry_key, Cached{j.s, j.bytes, j.res0, ++sv->tick, false}});
+      } else {
+        sv->resident -= j.bytes;
+        discard = j.s;
+      }
+      j.s = nullptr;
     }
-    j.s = nullptr;
+    j.done = true;
+    sv->completed++;
   }
-  j.done = true;
-  sv->completed++;
+  if (discard) a3d_solver_destroy(discard);
 }
 
 void scheduler(a3d_server* sv) {
@@ -245,28 +288,42 @@ void scheduler(a3d_server* sv) {
       sv->cv_work.wait_for(lk, std::chrono::milliseconds(50),
                            [&] { return sv->stop || !sv->pending.empty() || !sv->active.empty(); });
       if (sv->stop) break;
-      // admission: arrival order, slot cap and memory budget
-      size_t planned = sv->resident;
+      // admission: arrival order, slot cap and memory budget.  A request is warm only while an
+      // idle cached case of its geometry is still unpromised: it reserves that case (which
+      // then cannot be evicted) and adds no bytes; every other request adds its estimate,
+      // which must fit the budget once the unreserved idle cases are evicted.
+      size_t planned = sv->resident, idle = 0;
+      for (auto& c : sv->cache)
+        if (!c.second.reserved) idle += c.second.bytes;
       while (!sv->pending.empty() && (int)(sv->active.size() + admit.size()) < sv->cfg.max_active) {
         auto& j = sv->pending.front();
         const double est = request_bytes(j->req, sv->cfg.sequence);
-        const bool warm = sv->cfg.warm_start && sv->cache.count(j->req.geometry_key);
-        size_t idle = 0;
-        for (auto& c : sv->cache) idle += c.second.bytes;
-        if (!warm && planned + est > sv->cfg.hbm_budget_bytes + idle) break;  // wait for memory
-        if (!warm) planned += (size_t)est;
+        Cached* hit = nullptr;
+        if (sv->cfg.warm_start) {
+          auto range = sv->cache.equal_range(j->req.geometry_key);
+          for (auto it = range.first; it != range.second; ++it)
+            if (!it->second.reserved) { hit = &it->second; break; }
+        }
+        if (!hit && planned + est > sv->cfg.hbm_budget_bytes + idle) break;  // wait for memory
+        if (hit) {
+          hit->reserved = true;
+          idle -= hit->bytes;
+          j->planned_warm = true;
+        } else {
+          planned += (size_t)est;
+        }
         admit.push_back(j);
         sv->pending.pop_front();
       }
     }
     for (auto& j : admit) {
       j->t_admit = Clock::now();
-      std::lock_guard<std::mutex> lk(sv->mu);
       const int rc = start_case(sv, *j);
       if (rc != A3D_OK) {
         finish_case(sv, *j, rc);
         sv->cv_done.notify_all();
       } else {
+        std::lock_guard<std::mutex> lk(sv->mu);
         sv->active.push_back(j);
       }
     }
@@ -287,11 +344,16 @@ void scheduler(a3d_server* sv) {
       if (batch) a3d_batch_destroy(batch);
       batch = nullptr;
       if (a3d_batch_create(set.data(), (int)set.size(), &batch) != A3D_OK) {
-        std::lock_guard<std::mutex> lk(sv->mu);
-        sv->last_error = A3D_ERR_CUDA;
-        sv->last_error_msg = a3d_last_error();
+        {
+          std::lock_guard<std::mutex> lk(sv->mu);
+          sv->last_error = A3D_ERR_CUDA;
+          sv->last_error_msg = a3d_last_error();
+        }
         for (auto& j : act) finish_case(sv, *j, A3D_ERR_CUDA);
-        sv->active.clear();
+        {
+          std::lock_guard<std::mutex> lk(sv->mu);
+          sv->active.clear();
+        }
         sv->cv_done.notify_all();
         batch_key.clear();
         continue;
@@ -303,7 +365,10 @@ void scheduler(a3d_server* sv) {
     }
     int rc = a3d_batch_step(batch, sv->cfg.chunk_iters);
     if (rc == A3D_OK) rc = a3d_batch_sync(batch);
-    sv->rounds++;
+    {
+      std::lock_guard<std::mutex> lk(sv->mu);
+      sv->rounds++;
+    }
     std::vector<std::shared_ptr<Job>> still;
     for (auto& j : act) {
       double res = -1;
@@ -311,10 +376,8 @@ void scheduler(a3d_server* sv) {
       if (st == A3D_OK && j->coarse) {  // sequencing: the coarse case's own stopping rule
         if (j->coarse_res0 <= 0 && res > 0) j->coarse_res0 = res;
         if ((j->coarse_res0 > 0 && res / j->coarse_res0 <= sv->cfg.sequence_drop) ||
-            j->coarse->it >= sv->cfg.sequence_max_iters) {
-          std::lock_guard<std::mutex> lk(sv->mu);
+            j->coarse->it >= sv->cfg.sequence_max_iters)
           st = switch_to_target(sv, *j);
-        }
         if (st == A3D_OK) {
           still.push_back(j);
           continue;
@@ -328,7 +391,6 @@ void scheduler(a3d_server* sv) {
         fin = (j->res0 > 0 && res / j->res0 <= sv->cfg.residual_drop) || its >= sv->cfg.max_iters;
       }
       if (fin) {
-        std::lock_guard<std::mutex> lk(sv->mu);
         finish_case(sv, *j, st);
       } else {
         still.push_back(j);

@@ -206,6 +206,7 @@ void fill_stage_args(a3d_solver* s, StageArgs& a, const float* Qin, const float*
   a.NX = s->grid.NX; a.NY = s->grid.NY; a.NZ = s->grid.NZ;
   a.wa = wa; a.wb = wb; a.cfl = (float)s->cfl; a.order2 = s->order == 2;
   a.err = s->d_flag + 1;
+  a.wait_limit = s->wait_limit;
   a.kb = s->own_k0;
   a.ke = s->own_k1;
   for (int sd = 0; sd < 2; sd++) {
@@ -238,8 +239,9 @@ void fill_stage_args(a3d_solver* s, StageArgs& a, const float* Qin, const float*
 }
 
 int launch_stage(a3d_solver* s, const StageArgs& a) {
-  if (s->kernel == KERNEL_TMA || s->kernel == KERNEL_FUSED) {
+  if (s->kernel == KERNEL_TMA || s->kernel == KERNEL_FUSED || s->kernel == KERNEL_PAIR) {
     const int qin_buf = a.Qin == s->buf[0] ? 0 : a.Qin == s->buf[1] ? 1 : 2;
+    if (s->kernel == KERNEL_PAIR) return launch_pair(s, a, qin_buf, a.wa != 0.f);
     return s->kernel == KERNEL_FUSED ? launch_fused(s, a, qin_buf, a.wa != 0.f) : launch_tma(s, a, qin_buf, a.wa != 0.f);
   }
   if (s->kernel == KERNEL_MARCH) return launch_march(s, a);
@@ -463,12 +465,14 @@ extern "C" int a3d_solver_reset(a3d_solver* s) {
 
 namespace {
 
-// Number of pipelined z chunks a3d_solver_step uses: kernel 2 on a whole case only.  Automatic:
+// Number of pipelined z chunks a3d_solver_step uses: kernels 2 and 4 on a whole case only.  Automatic:
 // four chunks from 0.8M cells up, where a stage takes long enough to hide the extra stream and
 // event calls (measured: 4.1M-cell fighter 13.5 -> 15.1 G cell-updates/s, 1.0M-cell airliner
 // 10.1 -> 11.2), none below (0.6M-cell interceptor 8.4 -> 8.1 with four).
 int chunk_count(const a3d_solver* s) {
-  if (s->kernel != KERNEL_TMA || s->nbr[0] || s->nbr[1] || s->own_k0 != 0 || s->own_k1 != s->grid.NZ) return 1;
+  if ((s->kernel != KERNEL_TMA && s->kernel != KERNEL_PAIR) || s->nbr[0] || s->nbr[1] || s->own_k0 != 0 ||
+      s->own_k1 != s->grid.NZ)
+    return 1;
   const int runs = (s->grid.NZ + s->march_kz - 1) / s->march_kz;
   const int K = s->chunks_req > 0 ? s->chunks_req : (s->N >= 800000 ? 4 : 1);
   return std::max(1, std::min(K, std::min(runs, kMaxChunks)));
@@ -503,7 +507,8 @@ int step_chunked(a3d_solver* s, int n, int K) {
         }
         a.kb = kb[c];
         a.ke = ke[c];
-        A3D_TRY(launch_tma(s, a, qin_buf, stage == 1, s->cst[c]));
+        if (s->kernel == KERNEL_PAIR) A3D_TRY(launch_pair(s, a, qin_buf, stage == 1, s->cst[c]));
+        else A3D_TRY(launch_tma(s, a, qin_buf, stage == 1, s->cst[c]));
         A3D_CUDA(cudaEventRecord(s->cev[c][stage], s->cst[c]));
       }
       first = false;
@@ -571,7 +576,8 @@ extern "C" int a3d_solver_stage(a3d_solver* s, int32_t which) {
     const bool ok = which == 1 ? n->it == s->it
                                : ((n->it == s->it && n->phase == 1) || (n->it == s->it + 1 && n->phase == 0));
     A3D_ARG(ok, "neighbour slabs out of step");
-    A3D_ARG(s->kernel == KERNEL_CELL || s->kernel == KERNEL_TMA, "halo push needs stage kernel 0 or 2");
+    A3D_ARG(s->kernel == KERNEL_CELL || s->kernel == KERNEL_TMA || s->kernel == KERNEL_PAIR,
+            "halo push needs stage kernel 0, 2 or 4");
   }
   A3D_CUDA(cudaSetDevice(s->device));
   float *Q = s->buf[s->iQ], *S1 = s->buf[s->iS1], *B = s->buf[s->iB];
@@ -596,11 +602,12 @@ extern "C" int a3d_solver_stage(a3d_solver* s, int32_t which) {
 // that no copy is needed between stages.  lo / hi: the slabs below and above (either may be
 // null).  Every slab of the split must be given its neighbours; afterwards a slab advances
 // by a3d_solver_stage, with a3d_solver_sync_neighbors between the stages of all slabs.
-// Kernels 0 and 2 store only own planes and push; others are refused.
+// Kernels 0, 2 and 4 store only own planes and push; others are refused.
 extern "C" int a3d_solver_set_neighbors(a3d_solver* s, a3d_solver* lo, a3d_solver* hi) {
   clear_error();
   A3D_ARG(s && s != lo && s != hi, "null or self neighbour");
-  A3D_ARG(s->kernel == KERNEL_CELL || s->kernel == KERNEL_TMA, "halo push needs stage kernel 0 or 2");
+  A3D_ARG(s->kernel == KERNEL_CELL || s->kernel == KERNEL_TMA || s->kernel == KERNEL_PAIR,
+          "halo push needs stage kernel 0, 2 or 4");
   for (a3d_solver* n : {lo, hi}) {
     if (!n) continue;
     A3D_ARG(n->grid.NX == s->grid.NX && n->grid.NY == s->grid.NY, "neighbour differs in NX or NY");
@@ -745,8 +752,8 @@ extern "C" int a3d_solver_write(a3d_solver* s, const float* r, const float* ru, 
   return A3D_OK;
 }
 
-// Selects the stage kernel (0: per-cell, 1: z-march, 2: TMA, 3: fused) and the z planes per
-// CTA of the tiled kernels.  march_kz = 0 picks it for the TMA tile: 32 planes where that still
+// Selects the stage kernel (0: per-cell, 1: z-march, 2: TMA, 3: fused, 4: paired TMA) and the z
+// planes per CTA of the tiled kernels.  march_kz = 0 picks it for the TMA tiles: 32 planes where that still
 // launches four waves of CTAs (column tiles x z runs >= 4 x resident CTAs), else the longest run
 // of 16, 8 or 4 planes that launches two waves, else 2.  Shorter runs cost more ring prologue
 // per plane but keep the SMs busy and the z chunks of a3d_solver_step overlapping.  Measured
@@ -756,15 +763,17 @@ extern "C" int a3d_solver_write(a3d_solver* s, const float* r, const float* ru, 
 extern "C" int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t march_kz) {
   clear_error();
   A3D_ARG(s, "null solver");
-  A3D_ARG(kernel >= KERNEL_CELL && kernel <= KERNEL_FUSED, "kernel");
+  A3D_ARG(kernel >= KERNEL_CELL && kernel <= KERNEL_PAIR, "kernel");
   A3D_ARG(march_kz >= 0 && march_kz <= 1024, "march_kz");
   if (march_kz == 0) {
     march_kz = 16;
-    if (kernel == KERNEL_TMA) {
-      const long columns = (long)((s->grid.NX + 31) / 32) * ((s->grid.NY + 7) / 8);
+    if (kernel == KERNEL_TMA || kernel == KERNEL_PAIR) {
+      const int ty = kernel == KERNEL_PAIR ? 16 : 8;  // tile rows
+      const long columns = (long)((s->grid.NX + 31) / 32) * ((s->grid.NY + ty - 1) / ty);
       int resident = 0;
       A3D_CUDA(cudaSetDevice(s->device));
-      A3D_TRY(tma_resident_ctas(&resident));
+      if (kernel == KERNEL_PAIR) A3D_TRY(pair_resident_ctas(&resident));
+      else A3D_TRY(tma_resident_ctas(&resident));
       auto ctas = [&](int kz) { return columns * ((s->grid.NZ + kz - 1) / kz); };
       march_kz = 2;
       if (ctas(32) >= 4L * resident) march_kz = 32;
@@ -775,6 +784,17 @@ extern "C" int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t marc
   }
   s->kernel = kernel;
   s->march_kz = march_kz;
+  return A3D_OK;
+}
+
+// Try_waits a stage kernel spends on one TMA copy before it gives up, flags the solver and
+// leaves (A3D_WAIT_LIMIT_DEFAULT unless set; 0: at once).  A stage kernel that gives up makes
+// the next a3d_solver_sync, a3d_solver_read or reduction return A3D_ERR_TIMEOUT.  Not part of
+// the reference surface: it lets a test make a wait run out without anything faulting.
+extern "C" int a3d_solver_set_wait_limit(a3d_solver* s, uint32_t limit) {
+  clear_error();
+  A3D_ARG(s, "null solver");
+  s->wait_limit = limit;
   return A3D_OK;
 }
 
@@ -807,6 +827,10 @@ int check_kernel_error(a3d_solver* s) {
   A3D_CUDA(cudaMemcpyAsync(&f, s->d_flag + 1, sizeof(int), cudaMemcpyDeviceToHost, s->st));
   A3D_CUDA(cudaStreamSynchronize(s->st));
   if (f) {
+    // reported once: the flag is cleared, so that the solver can step again (the state of the
+    // failed stage is not meaningful; a caller resets it or loads a state)
+    A3D_CUDA(cudaMemsetAsync(s->d_flag + 1, 0, sizeof(int), s->st));
+    A3D_CUDA(cudaStreamSynchronize(s->st));
     set_error("a stage kernel gave up waiting for a TMA copy (bounded wait ran out)");
     return A3D_ERR_TIMEOUT;
   }

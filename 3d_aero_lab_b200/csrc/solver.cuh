@@ -28,6 +28,7 @@ struct StageArgs {
   float Pfix[3][5];               // primitive fixed states of types 3, 4, 5
   float Ufix[3][5];               // conservative fixed states written to fixed cells
   int* err;                       // set when a bounded wait inside a stage kernel ran out
+  uint32_t wait_limit;            // try_waits a stage kernel spends on one TMA copy before giving up
   // z slabs (kernels 0 and 2): planes this launch computes and stores, and the halo push
   int kb, ke;                     // [kb, ke): the solver's own planes (all planes unless split)
   float* peer[2];                 // lower/upper neighbour slab's buffer of the output role, or null
@@ -44,7 +45,7 @@ struct ForceList {
   void* block = nullptr;
 };
 
-enum StageKernel { KERNEL_CELL = 0, KERNEL_MARCH = 1, KERNEL_TMA = 2, KERNEL_FUSED = 3 };
+enum StageKernel { KERNEL_CELL = 0, KERNEL_MARCH = 1, KERNEL_TMA = 2, KERNEL_FUSED = 3, KERNEL_PAIR = 4 };
 constexpr int kMaxChunks = 4;  // z chunks of a pipelined step (6 or 8 measured no faster)
 
 }  // namespace a3d
@@ -66,9 +67,12 @@ struct a3d_solver {
   double cfl = 0.7;
   int order = 2;
   long it = 0;
-  int kernel = a3d::KERNEL_TMA;      // the fastest single-case stage kernel measured on B200
+  int kernel = a3d::KERNEL_PAIR;     // the fastest single-case stage kernel measured on B200
   CUtensorMap tmQ[3];             // TMA maps over the three state buffers
   CUtensorMap tmC;                // TMA map over the code array
+  CUtensorMap tmQp[3];            // the same maps with the paired tile's boxes (32 x 16 columns + halo)
+  CUtensorMap tmCp;
+  uint32_t wait_limit = A3D_WAIT_LIMIT_DEFAULT;  // try_waits a stage kernel spends on one TMA copy
   int march_kz = 16;              // z planes per CTA of the marching kernels
   // reductions
   double* d_red = nullptr;        // device partials + results
@@ -100,6 +104,10 @@ int build_force_list(a3d_solver* s);
 int make_tensor_maps(a3d_solver* s);
 int launch_tma(a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2, cudaStream_t st = nullptr);
 int launch_fused(a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2);
+int launch_pair(a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2, cudaStream_t st = nullptr);
+int make_pair_tensor_maps(a3d_solver* s);
+size_t pair_smem_bytes();
+int pair_resident_ctas(int* n);         // CTAs of the paired-tile stage kernel resident on the current device
 size_t fused_smem_bytes();
 size_t tma_smem_bytes();
 int tma_resident_ctas(int* n);          // CTAs of the TMA stage kernel resident on the current device

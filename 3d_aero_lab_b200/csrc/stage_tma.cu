@@ -37,7 +37,10 @@ void launch_mode(const a3d_solver* s, const StageArgs& a, int qin_buf, bool stag
   else k_stage_tma<false, MODE><<<grid, TX * TY, sm, st>>>(s->tmQ[qin_buf], s->tmC, a, s->march_kz);
 }
 
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+}  // namespace
+
+// The driver's tensor-map encoder, looked up once.
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   if (!fn) {
     cudaDriverEntryPointQueryResult q;
@@ -48,8 +51,6 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   }
   return fn;
 }
-
-}  // namespace
 
 // Three CTAs per SM need three tiles' shared memory (plus the 1 KB the hardware reserves per
 // CTA) within the SM's 228 KB.
@@ -69,7 +70,7 @@ int tma_resident_ctas(int* n) {
 
 // Tensor maps over the padded state buffers (x, y, z, component) and the code array (x, y, z).
 int make_tensor_maps(a3d_solver* s) {
-  auto enc = encode_fn();
+  auto enc = tensor_map_encoder();
   if (!enc) { set_error("cuTensorMapEncodeTiled is not available from the driver"); return A3D_ERR_CUDA; }
   const cuuint64_t NX = s->grid.NX, NY = s->grid.NY, NZ = s->grid.NZ, NXp = s->NXp;
   for (int b = 0; b < 3; b++) {
@@ -93,6 +94,7 @@ int make_tensor_maps(a3d_solver* s) {
   A3D_TRY((set_tma_attributes<true, 1>()));
   A3D_TRY((set_tma_attributes<false, 2>()));
   A3D_TRY((set_tma_attributes<true, 2>()));
+  A3D_TRY(make_pair_tensor_maps(s));
   return fused_set_attributes();
 }
 

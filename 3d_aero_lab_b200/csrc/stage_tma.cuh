@@ -142,13 +142,13 @@ __device__ __forceinline__ bool stage_tile(TmaSmem& S, const CUtensorMap* tmQ, c
   float Gz[5], Az = 1.f;
   {
     float Wa[5], Wm[5], Lm[5];
-    ok &= mbar_wait(&S.bar[slot_of(k0 - 2, k0)], parity_of(k0 - 2, k0));
+    ok &= mbar_wait(&S.bar[slot_of(k0 - 2, k0)], parity_of(k0 - 2, k0), a.wait_limit);
     slot_cell(a, S.slot[slot_of(k0 - 2, k0)], i, j, k0 - 2, i0, j0, Wa);
-    ok &= mbar_wait(&S.bar[slot_of(k0 - 1, k0)], parity_of(k0 - 1, k0));
+    ok &= mbar_wait(&S.bar[slot_of(k0 - 1, k0)], parity_of(k0 - 1, k0), a.wait_limit);
     cm = slot_cell(a, S.slot[slot_of(k0 - 1, k0)], i, j, k0 - 1, i0, j0, Wm);
-    ok &= mbar_wait(&S.bar[slot_of(k0, k0)], parity_of(k0, k0));
+    ok &= mbar_wait(&S.bar[slot_of(k0, k0)], parity_of(k0, k0), a.wait_limit);
     c0 = slot_cell(a, S.slot[slot_of(k0, k0)], i, j, k0, i0, j0, W0);
-    ok &= mbar_wait(&S.bar[slot_of(k0 + 1, k0)], parity_of(k0 + 1, k0));
+    ok &= mbar_wait(&S.bar[slot_of(k0 + 1, k0)], parity_of(k0 + 1, k0), a.wait_limit);
     c1 = slot_cell(a, S.slot[slot_of(k0 + 1, k0)], i, j, k0 + 1, i0, j0, W1);
 #pragma unroll
     for (int c = 0; c < 5; c++) Gz[c] = 0.f;
@@ -175,7 +175,7 @@ __device__ __forceinline__ bool stage_tile(TmaSmem& S, const CUtensorMap* tmQ, c
     const long qp = ((long)k * a.NY + j) * a.NXp + i;  // padded state index
     // ---- plane k+2 into the column window; plane k to shared memory ----
     const int sk = slot_of(k, k0), sk2 = slot_of(k + 2, k0);
-    ok = mbar_wait(&S.bar[sk2], parity_of(k + 2, k0));
+    ok = mbar_wait(&S.bar[sk2], parity_of(k + 2, k0), a.wait_limit);
     c2 = slot_cell(a, S.slot[sk2], i, j, k + 2, i0, j0, W2);
 #pragma unroll
     for (int v = 0; v < 5; v++) S.P[v][ty + 2][tx + 2] = W0[v];

@@ -10,7 +10,6 @@
 // a file-scope __device__ array as its scratch instead: the array is part of the loaded
 // module, so every GPU that loads the library holds it (about 96 KiB) until the process
 // exits, and no call allocates or frees anything.
-#include <mutex>
 #include "solver.cuh"
 
 namespace a3d {
@@ -26,28 +25,19 @@ constexpr int kScratchDoubles = 3 * kMaxBlocks + 3;               // partials, t
 // every partial it reads before reading it, so nothing has to start at zero.
 __device__ __align__(256) double g_force_scratch[kScratchDoubles];
 
-constexpr int kMaxDevices = 64;
-double* g_scratch_ptr[kMaxDevices] = {};
-std::mutex g_scratch_mu;
-
-// Device address of the scratch on the current device, looked up once per device.  In host
-// code `g_force_scratch` names a host-side shadow, not device memory, so it is never passed
-// to a kernel directly.
+// Device address of the scratch in the current context.  In host code `g_force_scratch` names a
+// host-side shadow, not device memory, so it is never passed to a kernel directly.  The address
+// is looked up on every call (a query that allocates nothing): a cached one would go stale if
+// the device were reset and the library's module loaded again at another address.  The first
+// call on a device may load the module, so it belongs before any stream capture.
 int scratch_for_current_device(double** out) {
-  int dev = 0;
-  A3D_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= kMaxDevices) { set_error("device index %d beyond %d", dev, kMaxDevices); return A3D_ERR_ARG; }
-  std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (!g_scratch_ptr[dev]) {
-    void* p = nullptr;
-    cudaError_t e = cudaGetSymbolAddress(&p, g_force_scratch);
-    if (e != cudaSuccess || !p) {
-      set_error("cudaGetSymbolAddress(force scratch) failed: %s", cudaGetErrorString(e));
-      return A3D_ERR_CUDA;
-    }
-    g_scratch_ptr[dev] = (double*)p;
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_force_scratch);
+  if (e != cudaSuccess || !p) {
+    set_error("cudaGetSymbolAddress(force scratch) failed: %s", cudaGetErrorString(e));
+    return A3D_ERR_CUDA;
   }
-  *out = g_scratch_ptr[dev];
+  *out = (double*)p;
   return A3D_OK;
 }
 

@@ -6,6 +6,7 @@
 #pragma once
 #include <cuda.h>
 #include <cstdint>
+#include "../../include/aero3d.h"
 
 namespace a3d {
 
@@ -66,10 +67,13 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
   return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity to complete.
-constexpr uint32_t kWaitLimit = 1u << 22;
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (uint32_t n = 0; n < kWaitLimit; n++)
+// Bounded wait for the phase with the given parity to complete: at most `limit` try_waits.
+// The stage kernels' main loops take the limit from StageArgs::wait_limit (a solver setting,
+// kWaitLimit by default); draining the copies in flight after a failed wait always uses
+// kWaitLimit, so that no copy lands in shared memory after its CTA has left.
+constexpr uint32_t kWaitLimit = A3D_WAIT_LIMIT_DEFAULT;
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, uint32_t limit = kWaitLimit) {
+  for (uint32_t n = 0; n < limit; n++)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }

@@ -5,7 +5,7 @@
  * grid generation, cut-cell geometry (volume fractions, face apertures, thin-wing
  * baffles, fixed-state engine cells), the SSP-RK2 solver object and the force,
  * Trefftz and residual post-processing.  The reference calls these from JavaScript;
- * a Node N-API shim binds these functions one to one (see INTEGRATION.md).
+ * a Node N-API shim binds these functions one to one.
  *
  * Conventions
  *  - Every function returns an int status (A3D_OK == 0).  No exception crosses the
@@ -40,6 +40,7 @@ extern "C" {
 #define A3D_ERR_NODEVICE   8  /* no CUDA device is visible                                */
 
 #define A3D_MAX_ENGINES 2
+#define A3D_WAIT_LIMIT_DEFAULT 4194304u  /* try_waits per TMA copy (a3d_solver_set_wait_limit) */
 #define A3D_MAX_EXITS   2
 #define A3D_ENV_N       300   /* nacelle envelope table intervals (src/air_cfd.js:53)   */
 
@@ -180,15 +181,25 @@ int a3d_solver_interp_state(a3d_solver* fine, const a3d_solver* coarse);
 /* Stage kernel selection; no counterpart in the reference (it has one shader).
  * kernel 0: one thread per cell evaluating its six faces (the reference's structure);
  * kernel 1: z-marching tiles that evaluate every face once, plain loads;
- * kernel 2 (default): the same fed by a TMA plane ring, three CTAs per SM;
+ * kernel 2: the same fed by a TMA plane ring, three CTAs per SM;
  * kernel 3: TMA ring, face states formed once per cell, paired f32x2 faces; results do
- *           not depend on the tiling.
- * march_kz = z planes per thread block; 0 (the default) picks for the TMA tile 32 planes if
+ *           not depend on the tiling;
+ * kernel 4 (default): TMA ring over 32 x 16-column tiles, each thread two x-adjacent cells
+ *           in packed f32x2 arithmetic, two CTAs per SM.
+ * march_kz = z planes per thread block; 0 (the default) picks for the TMA tiles 32 planes if
  * that still launches four waves of CTAs, else the longest of 16, 8 or 4 planes that
  * launches two waves, else 2.                                                            */
 int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t march_kz);
 int a3d_solver_get_kernel(a3d_solver* s, int32_t* kernel, int32_t* march_kz);
-/* Kernel 2 steps the case as up to 4 z chunks of whole z runs on their own streams, each
+/* Bounded device waits; no counterpart in the reference.  Every wait of a stage kernel (the
+ * TMA tiles, kernels 2 and 4) for a TMA plane copy gives up after `limit` tries
+ * (A3D_WAIT_LIMIT_DEFAULT unless set; 0 = give up at once): the kernel then waits, with the
+ * default limit, for its copies in flight, flags the solver and leaves, and the next
+ * a3d_solver_sync / read / reduction returns A3D_ERR_TIMEOUT once (the flag is then cleared;
+ * the state of the failed stage is not meaningful, reset or write it).  Limit 0 makes every
+ * wait run out without any fault, which is how the timeout path is tested.               */
+int a3d_solver_set_wait_limit(a3d_solver* s, uint32_t limit);
+/* Kernels 2 and 4 step the case as up to 4 z chunks of whole z runs on their own streams, each
  * chunk's stage waiting only for its neighbour chunks' previous stage: the tail of one stage
  * overlaps the start of the next.  0 = automatic (4 chunks from 0.8M cells up, else 1),
  * 1 = one launch per stage, 2..4 = that many chunks.  The results are the same bit for bit. */

@@ -25,21 +25,6 @@ def test_library_exports_every_declared_symbol(aero):
         assert hasattr(lib, n), n
 
 
-def test_integration_map_names_every_entry_point():
-    """Every declared function has a row in INTEGRATION.md's entry-point map, either by its full
-    name or in a family written as `a3d_batch_create/step/sync/...`."""
-    doc = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    named = set()
-    for tok in re.findall(r"`(a3d_[a-z_0-9]+(?:/[a-z_0-9]+)*)`", doc):
-        first, *rest = tok.split("/")
-        named.add(first)
-        if rest:
-            prefix = first[:first.index("_", 4) + 1]  # a3d_batch_create -> a3d_batch_
-            named.update(prefix + r for r in rest)
-    missing = [n for n in declared_functions() if n not in named]
-    assert not missing, missing
-
-
 def test_python_prototypes_cover_header():
     from importlib import import_module
     protos = import_module("3d_aero_lab_b200._lib").PROTOS

@@ -1,5 +1,6 @@
 """bench.py --impl reference on the host CPU: one JSON line with the contract's keys, the same
-workload config as the GPU arm, and under torchrun only rank 0 prints."""
+workload config as the GPU arm (its own step length in `step`), and under torchrun only rank 0
+prints."""
 import json
 import os
 import socket
@@ -31,7 +32,8 @@ def test_reference_arm_prints_one_contract_line():
     assert c["cells"] == c["dims"][0] * c["dims"][1] * c["dims"][2]
     assert 0.8 * 20000 < c["cells"] < 1.2 * 20000
     assert c["workload"].startswith("fighter plain solve, ") and c["fixed_states"] == "cycle at 0 m"
-    assert c["iterations_per_step"] == 2000
+    assert "iterations_per_step" not in c  # the step length is each arm's own: its `step` key
+    assert d["step"]["iterations"] == 1  # what the arm timed per step (--cpu-sample-iters)
 
 
 def test_reference_arm_under_torchrun_prints_on_rank_zero_only():

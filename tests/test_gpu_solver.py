@@ -39,7 +39,7 @@ def sig4(x):
     return float(f"{x:.4g}")
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 2, 3])
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4])
 def test_readme_case_matches_oracle_and_pin(aero, ref, kernel):
     ac, sh, og, ogeo, o = oracle_case(aero, ref, "fighter", 30000, 3.0)
     g, s = gpu_case(aero, sh, 30000, 3.0, kernel=kernel)
@@ -105,13 +105,14 @@ def test_batch_distribution_corners_match_oracle(aero, ref, typ, cells, M, alpha
     assert sig4(fg["CL"]) == sig4(fo["CL"]) and sig4(fg["CD"]) == sig4(fo["CD"])
 
 
+@pytest.mark.parametrize("kernel", [2, 4])
 @pytest.mark.parametrize("chunks", [0, 2, 3, 4])
-def test_pipelined_z_chunks_are_bit_identical(aero, chunks):
-    """The TMA kernel stepped as z chunks on their own streams, each waiting only for its
+def test_pipelined_z_chunks_are_bit_identical(aero, chunks, kernel):
+    """The TMA kernels stepped as z chunks on their own streams, each waiting only for its
     neighbour chunks, against one launch per stage."""
     sh = aero.shape_of(aero.build_aircraft("fighter"))
-    _, a = gpu_case(aero, sh, 400000, 3.0, kernel=2)
-    _, b = gpu_case(aero, sh, 400000, 3.0, kernel=2)
+    _, a = gpu_case(aero, sh, 400000, 3.0, kernel=kernel)
+    _, b = gpu_case(aero, sh, 400000, 3.0, kernel=kernel)
     a.set_chunks(1)
     b.set_chunks(chunks)
     for n in (1, 39):
@@ -122,6 +123,32 @@ def test_pipelined_z_chunks_are_bit_identical(aero, chunks):
     a.step(5)
     b.step(5)
     assert a.residual(1) == b.residual(1)
+
+
+@pytest.mark.parametrize("kernel", [2, 4])
+def test_bounded_wait_runs_out_reports_timeout_and_recovers(aero, kernel):
+    """The TMA tiles' bounded waits (SURVEY failure detection): with the wait limit at 0 every wait
+    for a plane copy gives up at once; the kernel drains its copies in flight, flags the solver
+    and leaves, nothing faults, and the host gets A3D_ERR_TIMEOUT once.  With the default limit
+    back and the state reset, the same solver steps exactly like a fresh one."""
+    from importlib import import_module
+    L = import_module("3d_aero_lab_b200._lib")
+    sh = aero.shape_of(aero.build_aircraft("fighter"))
+    _, s = gpu_case(aero, sh, 60000, 3.0, kernel=kernel)
+    _, fresh = gpu_case(aero, sh, 60000, 3.0, kernel=kernel)
+    s.set_wait_limit(0)
+    s.step(2)
+    with pytest.raises(L.AeroError) as e:
+        s.sync()
+    assert e.value.status == 7 and "bounded wait" in str(e.value)
+    s.sync()  # reported once: the flag is cleared
+    s.set_wait_limit(s.WAIT_LIMIT_DEFAULT)
+    s.reset()
+    s.step(10)
+    fresh.step(10)
+    assert np.array_equal(s.read_array(), fresh.read_array())
+    s.dispose()
+    fresh.dispose()
 
 
 def test_read_dt_is_the_last_iterations_local_time_step(aero):
@@ -150,7 +177,7 @@ def test_read_dt_is_the_last_iterations_local_time_step(aero):
     assert float(np.max(np.abs(dt[fluid] - ref[fluid]) / ref[fluid])) < 2e-6
 
 
-@pytest.mark.parametrize("kernel", [1, 2, 3])
+@pytest.mark.parametrize("kernel", [1, 2, 3, 4])
 def test_kernels_agree(aero, kernel):
     """The tiled kernels against the per-cell one (same float32 arithmetic, other summation order)."""
     sh = aero.shape_of(aero.build_aircraft("airliner"))
@@ -164,7 +191,7 @@ def test_kernels_agree(aero, kernel):
 
 @pytest.mark.parametrize("seed,dims,order", [(0, (9, 7, 6), 2), (1, (33, 9, 20), 2), (2, (40, 17, 3), 1),
                                              (3, (5, 2, 35), 2), (4, (64, 12, 18), 2)])
-@pytest.mark.parametrize("kernel", [0, 1, 2, 3])
+@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4])
 def test_random_boxes_per_cell(aero, ref, seed, dims, order, kernel):
     """Random cut cells, solids, fixed cells and baffles; every cell after 1 and 15 iterations."""
     rng = np.random.default_rng(seed)
