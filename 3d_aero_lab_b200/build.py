@@ -12,7 +12,8 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libaero3d.so")
-SOURCES = ["runtime.cu", "grid.cpp", "geom.cu", "solver.cu", "stage_march.cu", "stage_tma.cu", "stage_pair.cu", "stage_fused.cu", "batch.cu", "server.cpp", "reduce.cu", "sample.cu", "static_forces.cu", "interp.cu"]
+SOURCES = ["runtime.cu", "grid.cpp", "geom.cu", "solver.cu", "stage_tma.cu", "stage_pair.cu", "batch.cu", "server.cpp",
+           "reduce.cu", "sample.cu", "static_forces.cu", "interp.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
          "-ftz=true", "-prec-div=false", "-prec-sqrt=false", "-fmad=true", "--expt-relaxed-constexpr"]

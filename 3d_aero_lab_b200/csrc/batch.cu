@@ -5,8 +5,10 @@
 // counts; tiles of all cases are numbered consecutively (largest cases first).  The stage
 // kernel is persistent: a grid of (SM count x CTAs per SM) CTAs pulls tile numbers from a
 // global counter and runs the same tile as the single-case kernel: the TMA tile
-// (stage_tma.cuh, three CTAs per SM) for solvers on KERNEL_TMA, the packed fused tile
-// (stage_fused.cuh, two CTAs per SM) for solvers on KERNEL_FUSED.
+// (stage_tma.cuh, three CTAs per SM) for solvers on KERNEL_TMA, the paired-cell tile
+// (stage_pair.cuh, two CTAs per SM) for solvers on KERNEL_PAIR.  A tile's stage constants
+// are copied from the case table into shared memory, where the tile reads them as the
+// single-case kernel reads its kernel parameters, instead of holding them in registers.
 // The last CTA to find the queue empty resets the counter, so the four launches of two
 // SSP-RK2 iterations are captured once in a CUDA graph and replayed; buffer roles alternate
 // with the iteration's parity (Q and B swap every iteration, as in src/air_cfd.js:256).
@@ -20,15 +22,14 @@
 #include <algorithm>
 #include <numeric>
 #include <vector>
-#include "stage_fused.cuh"
+#include "stage_pair.cuh"
 #include "stage_tma.cuh"
 
 namespace a3d {
 
 namespace {
 
-using ring::TX;
-using ring::TY;
+constexpr int TILE_TMA = 0, TILE_PAIR = 1;
 
 struct __align__(128) BatchCase {
   CUtensorMap tmQ[3];  // maps over the case's three state buffers
@@ -44,12 +45,13 @@ struct __align__(128) BatchCase {
 // [2] its tile number, [3] how many tiles the CTA had finished before it.
 constexpr int kErrWords = 4;
 
-template <bool STAGE2, bool TMA_TILE>
+template <bool STAGE2, int TILE>
 __device__ __forceinline__ void batch_loop(unsigned char* smem_raw, const BatchCase* __restrict__ cases, int ncases,
                                            long long total, int parity, unsigned long long* counter,
                                            long long* err) {
   __shared__ long long s_w, s_done;  // ticket; tiles this CTA finished (kept out of registers)
   __shared__ int s_failed;
+  __shared__ StageArgs s_a;          // stage constants of the current tile's case
   if (threadIdx.x == 0) { s_done = 0; s_failed = 0; }
   for (;;) {
     if (threadIdx.x == 0) s_w = (long long)atomicAdd(counter, 1ULL);
@@ -75,10 +77,17 @@ __device__ __forceinline__ void batch_loop(unsigned char* smem_raw, const BatchC
     // stage 1: S1 = Q + dt R(Q); stage 2: B = Q/2 + (S1 + dt R(S1))/2
     const int qin = STAGE2 ? C.iS1 : iq;
     float* out = STAGE2 ? C.buf[ib] : C.buf[C.iS1];
-    const bool ok = TMA_TILE ? tma::stage_tile<STAGE2, true>(*reinterpret_cast<tma::TmaSmem*>(smem_raw), &C.tmQ[qin], &C.tmC,
-                                                       C.a, C.buf[iq], out, bx, by, bz, C.kz)
-                             : fused::stage_tile<STAGE2>(*reinterpret_cast<fused::FusedSmem*>(smem_raw), &C.tmQ[qin],
-                                                         &C.tmC, C.a, C.buf[iq], out, bx, by, bz, C.kz);
+    // Every thread of the CTA is past the previous tile (the two ticket barriers above), so
+    // thread 0 may overwrite the constants; the barrier after the copy publishes them before
+    // any thread reads them (a tile reads its dimensions and spacing arrays before its own
+    // opening barrier).
+    if (threadIdx.x == 0) s_a = C.a;
+    __syncthreads();
+    const bool ok = TILE == TILE_TMA
+                        ? tma::stage_tile<STAGE2, true>(*reinterpret_cast<tma::TmaSmem*>(smem_raw), &C.tmQ[qin], &C.tmC,
+                                                        s_a, C.buf[iq], out, bx, by, bz, C.kz)
+                        : pair::stage_tile<STAGE2, true>(*reinterpret_cast<pair::PairSmem*>(smem_raw), &C.tmQ[qin],
+                                                         &C.tmC, s_a, C.buf[iq], out, bx, by, bz, C.kz);
     if (!ok) {
       if (threadIdx.x == 0) {
         s_failed = 1;
@@ -95,19 +104,19 @@ __device__ __forceinline__ void batch_loop(unsigned char* smem_raw, const BatchC
 }
 
 template <bool STAGE2>
-__global__ void __launch_bounds__(TX * TY, 3)
+__global__ void __launch_bounds__(ring::TX * ring::TY, 3)
     k_batch_tma(const BatchCase* __restrict__ cases, int ncases, long long total, int parity,
                 unsigned long long* counter, long long* err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  batch_loop<STAGE2, true>(smem_raw, cases, ncases, total, parity, counter, err);
+  batch_loop<STAGE2, TILE_TMA>(smem_raw, cases, ncases, total, parity, counter, err);
 }
 
 template <bool STAGE2>
-__global__ void __launch_bounds__(TX * TY, 2)
-    k_batch_fused(const BatchCase* __restrict__ cases, int ncases, long long total, int parity,
-                  unsigned long long* counter, long long* err) {
+__global__ void __launch_bounds__(pair::NT, 2)
+    k_batch_pair(const BatchCase* __restrict__ cases, int ncases, long long total, int parity,
+                 unsigned long long* counter, long long* err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
-  batch_loop<STAGE2, false>(smem_raw, cases, ncases, total, parity, counter, err);
+  batch_loop<STAGE2, TILE_PAIR>(smem_raw, cases, ncases, total, parity, counter, err);
 }
 
 }  // namespace
@@ -129,7 +138,7 @@ struct a3d_batch {
   long long total = 0;
   int kz = 32;
   int ctas_per_sm = 2;
-  bool tma_tile = true;            // TMA tile (KERNEL_TMA solvers) or packed fused tile
+  bool tma_tile = true;            // TMA tile (KERNEL_TMA solvers) or paired-cell tile (KERNEL_PAIR)
   cudaGraphExec_t graph = nullptr;
   bool table_dirty = true;
   // mode 1: every case's own single-case stage launches, each case on its own forked stream,
@@ -164,8 +173,10 @@ int build_table(a3d_batch* b) {
   for (int r = 0; r < n; r++) {
     a3d_solver* s = b->solvers[b->order[r]];
     BatchCase& C = b->h_cases[r];
-    C.tmQ[0] = s->tmQ[0]; C.tmQ[1] = s->tmQ[1]; C.tmQ[2] = s->tmQ[2];
-    C.tmC = s->tmC;
+    const bool pt = !b->tma_tile;  // the paired tile's maps have its 32 x 16-column boxes
+    for (int k = 0; k < 3; k++) C.tmQ[k] = pt ? s->tmQp[k] : s->tmQ[k];
+    C.tmC = pt ? s->tmCp : s->tmC;
+    const int TX = 32, TY = pt ? pair::TY : ring::TY;
     fill_stage_args(s, C.a, nullptr, nullptr, nullptr, 0.5f, 0.5f);
     for (int k = 0; k < 3; k++) C.buf[k] = s->buf[k];
     C.iQ = s->iQ; C.iS1 = s->iS1; C.iB = s->iB;
@@ -182,17 +193,19 @@ int build_table(a3d_batch* b) {
   return A3D_OK;
 }
 
-int launch_pair(a3d_batch* b, int parity, cudaStream_t st) {
+// The two persistent stage launches of one iteration (buffer roles of the given parity).
+int launch_iteration(a3d_batch* b, int parity, cudaStream_t st) {
   const int grid = b->n_sm * b->ctas_per_sm, n = (int)b->solvers.size();
   unsigned long long* c0 = b->d_counters + 2 * parity;
   if (b->tma_tile) {
     const size_t smem = tma_smem_bytes();
-    k_batch_tma<false><<<grid, TX * TY, smem, st>>>(b->d_cases, n, b->total, parity, c0, b->d_err);
-    k_batch_tma<true><<<grid, TX * TY, smem, st>>>(b->d_cases, n, b->total, parity, c0 + 1, b->d_err);
+    const int nt = ring::TX * ring::TY;
+    k_batch_tma<false><<<grid, nt, smem, st>>>(b->d_cases, n, b->total, parity, c0, b->d_err);
+    k_batch_tma<true><<<grid, nt, smem, st>>>(b->d_cases, n, b->total, parity, c0 + 1, b->d_err);
   } else {
-    const size_t smem = fused_smem_bytes();
-    k_batch_fused<false><<<grid, TX * TY, smem, st>>>(b->d_cases, n, b->total, parity, c0, b->d_err);
-    k_batch_fused<true><<<grid, TX * TY, smem, st>>>(b->d_cases, n, b->total, parity, c0 + 1, b->d_err);
+    const size_t smem = pair_smem_bytes();
+    k_batch_pair<false><<<grid, pair::NT, smem, st>>>(b->d_cases, n, b->total, parity, c0, b->d_err);
+    k_batch_pair<true><<<grid, pair::NT, smem, st>>>(b->d_cases, n, b->total, parity, c0 + 1, b->d_err);
   }
   A3D_CUDA(cudaGetLastError());
   return A3D_OK;
@@ -203,8 +216,8 @@ int build_graph(a3d_batch* b) {
   free_graph(b);
   cudaGraph_t g = nullptr;
   A3D_CUDA(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
-  int rc = launch_pair(b, 0, b->st);
-  if (rc == A3D_OK) rc = launch_pair(b, 1, b->st);
+  int rc = launch_iteration(b, 0, b->st);
+  if (rc == A3D_OK) rc = launch_iteration(b, 1, b->st);
   cudaError_t e = cudaStreamEndCapture(b->st, &g);
   if (rc != A3D_OK) { if (g) cudaGraphDestroy(g); return rc; }
   if (e != cudaSuccess) { set_error("graph capture: %s", cudaGetErrorString(e)); return A3D_ERR_CUDA; }
@@ -307,7 +320,7 @@ int run(a3d_batch* b, int n) {
   if (b->table_dirty) A3D_TRY(build_table(b));
   if (!b->graph) A3D_TRY(build_graph(b));
   for (int p = 0; p + 1 < n; p += 2) A3D_CUDA(cudaGraphLaunch(b->graph, b->st));
-  if (n & 1) A3D_TRY(launch_pair(b, 0, b->st));
+  if (n & 1) A3D_TRY(launch_iteration(b, 0, b->st));
   A3D_CUDA(cudaEventRecord(b->ev_out, b->st));
   for (a3d_solver* s : b->solvers) {
     A3D_CUDA(cudaStreamWaitEvent(s->st, b->ev_out, 0));
@@ -337,7 +350,8 @@ extern "C" int a3d_batch_create(a3d_solver* const* solvers, int32_t n, a3d_batch
     A3D_ARG(solvers[k]->own_k0 == 0 && solvers[k]->own_k1 == solvers[k]->grid.NZ && !solvers[k]->nbr[0] &&
                 !solvers[k]->nbr[1],
             "z-slab solvers cannot be batched");
-    A3D_ARG(solvers[k]->kernel == KERNEL_FUSED || solvers[k]->kernel == KERNEL_TMA, "batch needs TMA-capable solvers");
+    A3D_ARG(solvers[k]->kernel == KERNEL_PAIR || solvers[k]->kernel == KERNEL_TMA,
+            "batch needs solvers on a TMA tile (stage kernel 2 or 4)");
     A3D_ARG(solvers[k]->kernel == solvers[0]->kernel, "all solvers of a batch must select the same stage kernel");
   }
   A3D_CUDA(cudaSetDevice(dev));
@@ -365,9 +379,11 @@ extern "C" int a3d_batch_create(a3d_solver* const* solvers, int32_t n, a3d_batch
   if (e == cudaSuccess) e = cudaMemsetAsync(b->d_err, 0, kErrWords * sizeof(long long), b->st);
   if (e != cudaSuccess) { set_error("batch setup: %s", cudaGetErrorString(e)); rc = e == cudaErrorMemoryAllocation ? A3D_ERR_NOMEM : A3D_ERR_CUDA; }
   if (rc == A3D_OK) {
-    const int ft = (int)fused_smem_bytes(), tt = (int)tma_smem_bytes();
-    int r = cudaFuncSetAttribute(k_batch_fused<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ft);
-    if (r == cudaSuccess) r = cudaFuncSetAttribute(k_batch_fused<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ft);
+    const int pt = (int)pair_smem_bytes(), tt = (int)tma_smem_bytes();
+    int r = cudaFuncSetAttribute(k_batch_pair<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, pt);
+    if (r == cudaSuccess) r = cudaFuncSetAttribute(k_batch_pair<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, pt);
+    if (r == cudaSuccess) r = cudaFuncSetAttribute(k_batch_pair<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    if (r == cudaSuccess) r = cudaFuncSetAttribute(k_batch_pair<true>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     if (r == cudaSuccess) r = cudaFuncSetAttribute(k_batch_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, tt);
     if (r == cudaSuccess) r = cudaFuncSetAttribute(k_batch_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, tt);
     if (r == cudaSuccess) r = cudaFuncSetAttribute(k_batch_tma<false>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);

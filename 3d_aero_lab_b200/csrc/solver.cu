@@ -9,10 +9,12 @@
 // the base state Q in both stages, as the reference's shader does (CFD3_FS :357-359); it is
 // the value CfdCPU stores in stage 1 and reuses.
 //
-// Two stage kernels are built:
-//   KERNEL_CELL  - one thread per cell, six faces per cell, the reference's structure;
-//   KERNEL_MARCH - CTA tile of 32 x 8 columns marching in z, every face flux computed
-//                  once per tile and shared through shared memory (stage_march.cuh).
+// Three stage kernels are built:
+//   KERNEL_CELL - one thread per cell, six faces per cell, the reference's structure (here);
+//   KERNEL_TMA  - CTA tile of 32 x 8 columns marching in z, every face flux computed once per
+//                 tile, planes staged by a TMA ring (stage_tma.cuh);
+//   KERNEL_PAIR - the same marching over 32 x 16 columns, each thread two x-adjacent cells in
+//                 packed f32x2 arithmetic (stage_pair.cuh), the default.
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -197,7 +199,6 @@ void prim_of(const double U[5], float P[5]) {  // cfdPrim5 in float64, rounded t
 
 }  // namespace
 
-int launch_march(a3d_solver* s, const StageArgs& a);  // stage_march.cu
 
 void fill_stage_args(a3d_solver* s, StageArgs& a, const float* Qin, const float* B, float* Out, float wa, float wb) {
   a.Qin = Qin; a.B = B; a.Out = Out; a.Np = s->Np; a.NXp = s->NXp;
@@ -239,12 +240,11 @@ void fill_stage_args(a3d_solver* s, StageArgs& a, const float* Qin, const float*
 }
 
 int launch_stage(a3d_solver* s, const StageArgs& a) {
-  if (s->kernel == KERNEL_TMA || s->kernel == KERNEL_FUSED || s->kernel == KERNEL_PAIR) {
+  if (s->kernel == KERNEL_TMA || s->kernel == KERNEL_PAIR) {
     const int qin_buf = a.Qin == s->buf[0] ? 0 : a.Qin == s->buf[1] ? 1 : 2;
     if (s->kernel == KERNEL_PAIR) return launch_pair(s, a, qin_buf, a.wa != 0.f);
-    return s->kernel == KERNEL_FUSED ? launch_fused(s, a, qin_buf, a.wa != 0.f) : launch_tma(s, a, qin_buf, a.wa != 0.f);
+    return launch_tma(s, a, qin_buf, a.wa != 0.f);
   }
-  if (s->kernel == KERNEL_MARCH) return launch_march(s, a);
   k_stage_cell<<<(unsigned)((s->N + 255) / 256), 256, 0, s->st>>>(a);
   A3D_CUDA(cudaGetLastError());
   return A3D_OK;
@@ -752,8 +752,8 @@ extern "C" int a3d_solver_write(a3d_solver* s, const float* r, const float* ru, 
   return A3D_OK;
 }
 
-// Selects the stage kernel (0: per-cell, 1: z-march, 2: TMA, 3: fused, 4: paired TMA) and the z
-// planes per CTA of the tiled kernels.  march_kz = 0 picks it for the TMA tiles: 32 planes where that still
+// Selects the stage kernel (0: per-cell, 2: TMA tile, 4: paired-cell TMA tile) and the z planes
+// per CTA of the tiled kernels.  march_kz = 0 picks it for the TMA tiles: 32 planes where that still
 // launches four waves of CTAs (column tiles x z runs >= 4 x resident CTAs), else the longest run
 // of 16, 8 or 4 planes that launches two waves, else 2.  Shorter runs cost more ring prologue
 // per plane but keep the SMs busy and the z chunks of a3d_solver_step overlapping.  Measured
@@ -763,7 +763,7 @@ extern "C" int a3d_solver_write(a3d_solver* s, const float* r, const float* ru, 
 extern "C" int a3d_solver_set_kernel(a3d_solver* s, int32_t kernel, int32_t march_kz) {
   clear_error();
   A3D_ARG(s, "null solver");
-  A3D_ARG(kernel >= KERNEL_CELL && kernel <= KERNEL_PAIR, "kernel");
+  A3D_ARG(kernel == KERNEL_CELL || kernel == KERNEL_TMA || kernel == KERNEL_PAIR, "kernel must be 0, 2 or 4");
   A3D_ARG(march_kz >= 0 && march_kz <= 1024, "march_kz");
   if (march_kz == 0) {
     march_kz = 16;

@@ -45,7 +45,9 @@ struct ForceList {
   void* block = nullptr;
 };
 
-enum StageKernel { KERNEL_CELL = 0, KERNEL_MARCH = 1, KERNEL_TMA = 2, KERNEL_FUSED = 3, KERNEL_PAIR = 4 };
+// Stage kernels by number (the numbers 1 and 3 belonged to two tiles since retired: slower
+// than the TMA tiles on every measured case).
+enum StageKernel { KERNEL_CELL = 0, KERNEL_TMA = 2, KERNEL_PAIR = 4 };
 constexpr int kMaxChunks = 4;  // z chunks of a pipelined step (6 or 8 measured no faster)
 
 }  // namespace a3d
@@ -103,14 +105,11 @@ void fill_stage_args(a3d_solver* s, StageArgs& a, const float* Qin, const float*
 int build_force_list(a3d_solver* s);
 int make_tensor_maps(a3d_solver* s);
 int launch_tma(a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2, cudaStream_t st = nullptr);
-int launch_fused(a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2);
 int launch_pair(a3d_solver* s, const StageArgs& a, int qin_buf, bool stage2, cudaStream_t st = nullptr);
 int make_pair_tensor_maps(a3d_solver* s);
 size_t pair_smem_bytes();
 int pair_resident_ctas(int* n);         // CTAs of the paired-tile stage kernel resident on the current device
-size_t fused_smem_bytes();
 size_t tma_smem_bytes();
 int tma_resident_ctas(int* n);          // CTAs of the TMA stage kernel resident on the current device
-int fused_set_attributes();
 int check_kernel_error(a3d_solver* s);  // A3D_ERR_TIMEOUT if a stage kernel flagged a timeout
 }  // namespace a3d

@@ -94,8 +94,7 @@ int make_tensor_maps(a3d_solver* s) {
   A3D_TRY((set_tma_attributes<true, 1>()));
   A3D_TRY((set_tma_attributes<false, 2>()));
   A3D_TRY((set_tma_attributes<true, 2>()));
-  A3D_TRY(make_pair_tensor_maps(s));
-  return fused_set_attributes();
+  return make_pair_tensor_maps(s);
 }
 
 // The stage kernel over planes [a.kb, a.ke) on stream st (the solver's stream by default).

@@ -23,6 +23,7 @@ from .aircraft import build_aircraft, shape_of, trefftz_x
 from .cfd import CfdGPU, cfd_grid, freestream
 
 TYPES = ("airliner", "interceptor", "fighter")
+SERVED_KERNEL = 2  # the stage kernel the server configures its cases with (server.cpp configure_case)
 _AIRCRAFT = {}
 
 
@@ -148,17 +149,34 @@ def poisson_run(server, reqs, rate, seed, timeout=1800.0):
     return res, wall
 
 
-def latency_stats(res):
-    lat = np.array([r["t_done"] - r["t_submit"] for r in res])
-    return {"p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
-            "mean_s": float(lat.mean()), "max_s": float(lat.max())}
+def converged(r, residual_drop=1e-3):
+    """True when a result stopped on the residual drop, False when it stopped at the cap."""
+    return bool(r["res0"] and r["res0"] > 0 and r["residual"] is not None and r["residual"] / r["res0"] <= residual_drop)
 
 
-def solve_plain(r, residual_drop=1e-3, chunk=50, max_iters=3000, device=0, kernel=2, kz=0, chunks=0):
+def latency_stats(res, residual_drop=None):
+    """p50/p99/mean/max latency (submit to result).  With residual_drop, also the fraction of
+    requests that met the drop and the same statistics over converged and capped requests
+    separately (None where a group is empty)."""
+    def stats(rs):
+        if not rs:
+            return None
+        lat = np.array([r["t_done"] - r["t_submit"] for r in rs])
+        return {"n": len(rs), "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99)),
+                "mean_s": float(lat.mean()), "max_s": float(lat.max())}
+    out = stats(res)
+    if residual_drop is not None:
+        conv = [r for r in res if converged(r, residual_drop)]
+        capped = [r for r in res if not converged(r, residual_drop)]
+        out.update({"converged_fraction": len(conv) / len(res), "converged": stats(conv), "capped": stats(capped)})
+    return out
+
+
+def solve_plain(r, residual_drop=1e-3, chunk=50, max_iters=3000, device=0, kernel=4, kz=0, chunks=0):
     """One request on its own solver, the same convergence rule as the server.  By default the
-    lone case's fastest configuration (z run and z chunks picked from its size); with the
-    server's per-case configuration (kz=16, chunks=1) the results equal the served ones bit for
-    bit."""
+    lone case's fastest configuration (the default stage kernel, z run and z chunks picked from
+    its size); with the server's per-case configuration (kernel=SERVED_KERNEL, kz=16, chunks=1)
+    the results equal the served ones bit for bit."""
     ac, sh = aircraft(r["type"])
     g = cfd_grid(sh, r["cells"])
     s = CfdGPU(g, shape=sh, delta=r["delta"], device=device)

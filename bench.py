@@ -37,7 +37,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 ALG_BYTES_PER_CELL_UPDATE = 142
-KERNEL_NAMES = {0: "k_stage_cell", 1: "k_stage_march", 2: "k_stage_tma", 3: "k_stage_fused", 4: "k_stage_pair"}
+KERNEL_NAMES = {0: "k_stage_cell", 2: "k_stage_tma", 4: "k_stage_pair"}
 
 
 def measured_traffic(kernel, cells):
@@ -81,14 +81,17 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--batch-cases", type=int, default=64)
     p.add_argument("--batch-iters", type=int, default=1000)
-    p.add_argument("--serve-requests", type=int, default=32)
+    p.add_argument("--serve-requests", type=int, default=200)
     p.add_argument("--serve-rate", type=float, default=20.0)
-    p.add_argument("--serve-sequence", type=int, default=8)
+    p.add_argument("--serve-sequence", type=int, default=0,
+                   help="also serve the same arrivals with grid sequencing (coarse case at cells/S first)")
     p.add_argument("--split", type=int, default=0,
                    help="also time the case cut into this many z slabs: on one GPU in one process, or "
                         "under torchrun one slab per rank (halo planes by NCCL send/recv)")
     p.add_argument("--no-batch", action="store_true")
     p.add_argument("--no-serve", action="store_true")
+    p.add_argument("--no-c5", action="store_true", help="skip the 120M-cell airliner leg")
+    p.add_argument("--c5-iters", type=int, default=200)
     return p.parse_args()
 
 
@@ -219,6 +222,41 @@ def cpu_baseline(aero, args, ac, iters, threads):
     return g.N * iters / dt, g.N
 
 
+def bench_c5(aero, args, ws, rank, local):
+    """C5: the twin-engine airliner half model at ~120M cells (under-wing nacelle intake-sink,
+    bypass and core-jet cells holding the engine field model's 11 km states), M0.78, alpha 2.5,
+    delta 0, at a reduced iteration count: cell-updates/s from CUDA events on the solver stream,
+    the stage time alone and its HBM roofline (71 algorithmic bytes per cell and stage)."""
+    import torch
+    case = aero.Case(aircraft_type="airliner", cells=1.2e8, M=0.78, alpha=2.5, delta=0.0, device=local,
+                     fixed="cycle", h=11000.0)
+    s, g, it = case.solver, case.g, args.c5_iters
+    tuning = {"kernel": KERNEL_NAMES[s.kernel()[0]], "march_kz": s.kernel()[1], "z_chunks": s.chunks()}
+    stream = torch.cuda.ExternalStream(s.stream, device=torch.device("cuda", local))
+    s.step(2)  # warm-up
+    s.reset()
+    s.sync()
+    barrier(ws)
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record(stream)
+    s.step(it)
+    e1.record(stream)
+    f = case.forces()
+    e2.record(stream)
+    e2.synchronize()
+    ms_step = max_over_ranks(e0.elapsed_time(e1), ws)
+    s.dispose()
+    peak, peak_kind = peaks()
+    stage_ms = ms_step / (2 * it)
+    achieved = ALG_BYTES_PER_CELL_UPDATE / 2 * g.N / (stage_ms * 1e-3) / 1e9
+    return {"workload": f"airliner plain solve, {g.NX}x{g.NY}x{g.NZ} = {g.N} cells, M0.78 a2.5 d0, cycle fixed "
+                        f"states at 11 km, {it} SSP-RK2 iterations", "cells": g.N,
+            "cell_updates_per_s": ws * g.N * it / (ms_step * 1e-3), "ms_per_iteration": ms_step / it,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": peak_kind, "stage_ms": stage_ms},
+            "tuning": tuning, "CL": f["CL"], "CD": f["CD"]}
+
+
 def bench_batched(aero, args, ws, rank, local):
     """C3: seeded cases of uneven size, all advanced together (concurrent per-case launches or one
     persistent launch per RK stage, in a CUDA graph, mode and schedule autotuned) vs the same cases solved one after another (plain loop).
@@ -230,7 +268,7 @@ def bench_batched(aero, args, ws, rank, local):
     for r in reqs:
         c = aero.Case(aircraft_type=r["type"], cells=r["cells"], M=r["M"], alpha=r["alpha"], delta=r["delta"],
                       device=local, fixed=r["fix"])
-        c.solver.set_kernel(2, 0)  # plain loop: each lone case's fastest z run and z chunks
+        c.solver.set_kernel(4, 0)  # plain loop: each lone case's fastest kernel, z run and z chunks
         cases.append(c)
     cells = sum(c.g.N for c in cases)
     it = args.batch_iters
@@ -282,7 +320,7 @@ def bench_served(aero, args, ws, rank, local):
     res, wall = serve.poisson_run(sv, reqs, args.serve_rate / ws, seed=7 + rank)
     st = sv.stats()
     sv.close()
-    lat = serve.latency_stats(res)
+    lat = serve.latency_stats(res, 1e-3)
     span = max(r["t_done"] for r in res) - min(r["t_submit"] for r in res)
     seq = None
     if args.serve_sequence > 1:  # the same arrivals with grid sequencing (coarse case at cells/8 first)
@@ -299,7 +337,7 @@ def bench_served(aero, args, ws, rank, local):
                "mean_final_residual_ratio": statistics.fmean([r["residual"] / r["res0"] for r in sres if r["res0"] > 0]),
                "max_abs_dCL_vs_unsequenced": max((abs(a["CL"] - b["CL"]) for a, b in cold), default=None)}
     plain, _ = serve.plain_loop(reqs, args.serve_rate / ws, seed=7 + rank)
-    plat = serve.latency_stats([dict(r, t_done=r["t_done"], t_submit=r["t_submit"]) for r in plain])
+    plat = serve.latency_stats(plain, 1e-3)
     pspan = max(r["t_done"] for r in plain) - min(r["t_submit"] for r in plain)
     span = max_over_ranks(span, ws)
     pspan = max_over_ranks(pspan, ws)
@@ -307,8 +345,11 @@ def bench_served(aero, args, ws, rank, local):
     return {"workload": f"{args.serve_requests} requests, Poisson {args.serve_rate}/s (seed 7), C3 distribution with "
                         f"{max(4, args.serve_requests // 3)} distinct geometries, residual drop 1e-3 or 3000 iterations",
             "solves_per_s": args.serve_requests / span, "p50_s": lat["p50_s"], "p99_s": lat["p99_s"],
+            "converged_fraction": lat["converged_fraction"], "latency_converged": lat["converged"],
+            "latency_capped": lat["capped"],
             "plain_loop_solves_per_s": args.serve_requests / pspan, "plain_p50_s": plat["p50_s"],
-            "plain_p99_s": plat["p99_s"], "speedup_vs_plain": pspan / span,
+            "plain_p99_s": plat["p99_s"], "plain_converged_fraction": plat["converged_fraction"],
+            "speedup_vs_plain": pspan / span,
             "warm_starts": st["warm_starts"], "rounds": st["rounds"],
             "mean_iterations": float(sum(r["iterations"] for r in res) / len(res)),
             "mean_final_residual_ratio": statistics.fmean([r["residual"] / r["res0"] for r in res if r["res0"] > 0]),
@@ -478,6 +519,11 @@ def main():
     e2e_ms = max_over_ranks(t0.elapsed_time(t1) / args.steps, ws)
     s.dispose()
     extra = {}
+    if not args.no_c5:
+        try:
+            extra["c5"] = bench_c5(aero, args, ws, rank, local)
+        except Exception as e:  # reported, not hidden
+            extra["c5"] = {"error": repr(e)}
     if args.split:
         try:
             extra["split"] = bench_split(aero, args, ws, rank, local)

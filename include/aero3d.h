@@ -180,12 +180,11 @@ int a3d_solver_sample(a3d_solver* s, int32_t n, const double* xyz, double* out5,
 int a3d_solver_interp_state(a3d_solver* fine, const a3d_solver* coarse);
 /* Stage kernel selection; no counterpart in the reference (it has one shader).
  * kernel 0: one thread per cell evaluating its six faces (the reference's structure);
- * kernel 1: z-marching tiles that evaluate every face once, plain loads;
- * kernel 2: the same fed by a TMA plane ring, three CTAs per SM;
- * kernel 3: TMA ring, face states formed once per cell, paired f32x2 faces; results do
- *           not depend on the tiling;
- * kernel 4 (default): TMA ring over 32 x 16-column tiles, each thread two x-adjacent cells
+ * kernel 2: z-marching 32 x 8-column tiles that evaluate every face once, fed by a TMA
+ *           plane ring, three CTAs per SM;
+ * kernel 4 (default): the same over 32 x 16-column tiles, each thread two x-adjacent cells
  *           in packed f32x2 arithmetic, two CTAs per SM.
+ * (Numbers 1 and 3 belonged to two tiles since retired; they are refused.)
  * march_kz = z planes per thread block; 0 (the default) picks for the TMA tiles 32 planes if
  * that still launches four waves of CTAs, else the longest of 16, 8 or 4 planes that
  * launches two waves, else 2.                                                            */

@@ -8,12 +8,17 @@ bar of the reference's own GPU/CPU check:
   * max|gpu - cpu| / max|cpu| per variable (tools/gpucmp.mjs:19-21) <= 3e-6 for all five;
   * per-cell relative difference <= 3e-6 for rho and E (the variables that never cross zero);
   * C_L and C_D agree to 4 significant digits.
-The default 60 iterations keep the oracle near 10 s; A3D_C2_PARITY_ITERS=2000 runs the bench's
-full solve (about 15 minutes of oracle time) with the same assertions.
+The 60 iterations keep the oracle near 10 s.  Over the bench's full 2000 iterations two float32
+runs of the scheme drift apart by rounding (about 1e-5, whatever the implementation: the
+oracle's own float32 run sits that far from its FP64 run), so the full solve is checked against
+the FP64 run instead: A3D_C2_LONG=1 runs it (about 12 minutes of oracle time) and asserts that
+the GPU solution is no further from the FP64 solution than the reference's own float32 CPU
+path is, with C_L and C_D to 4 significant digits across all three runs.
 
 C5 - the twin-engine airliner at ~120M cells with its under-wing nacelle's intake-sink, bypass
 and core-jet cells (src/air_cfd.js:117-131) holding the 11 km cycle states, M0.78, alpha 2.5:
-two iterations against the oracle, then forces and Trefftz drag from one state on both sides.
+two iterations against the oracle, then forces and Trefftz drag from one (perturbed) state on
+both sides.
 """
 import math
 import os
@@ -54,7 +59,7 @@ def compare(Qg, Qo):
 
 
 def test_c2_fighter_4m_matches_oracle(aero, ref):
-    its = int(os.environ.get("A3D_C2_PARITY_ITERS", "60"))
+    its = 60
     ac, g, o, s = cases(aero, ref, "fighter", 4.0e6, 0.6, 3.0, 3.0, 0.0)
     assert (g.NX, g.NY, g.NZ) == (311, 108, 123)
     assert s.kernel()[0] == 4  # the default stage kernel, the one the bench times
@@ -69,6 +74,38 @@ def test_c2_fighter_4m_matches_oracle(aero, ref):
     fg = s.forces(3.0, 0.6, r["S"], r["xcg"], 0.0, r["c"])
     fo = o.forces(3.0, 0.6, r["S"], r["xcg"], 0.0, r["c"])
     assert sig4(fg["CL"]) == sig4(fo["CL"]) and sig4(fg["CD"]) == sig4(fo["CD"]), (fg, fo)
+    s.dispose()
+
+
+@pytest.mark.skipif(os.environ.get("A3D_C2_LONG") != "1", reason="12 minutes of oracle time: set A3D_C2_LONG=1")
+def test_c2_full_solve_is_as_accurate_as_the_reference_cpu_path(aero, ref):
+    its = 2000
+    ac, g, o32, s = cases(aero, ref, "fighter", 4.0e6, 0.6, 3.0, 3.0, 0.0)
+    s.step(its)
+    o32.step(its)
+    Qg, Q32 = s.read_array(), o32.read()
+    del o32
+    sh = aero.shape_of(ac)
+    o64 = ref.CfdCPU(g, ref.geom(sh, g, 3.0), prec=64, threads=ref.max_threads())
+    F = freestream(0.6, 3.0)
+    o64.setFree(F)
+    o64.setFix(aero.fix_states(ac, 0.0, 0.6, 3.0)[1])
+    o64.reset()
+    o64.step(its)
+    Q64 = o64.read()
+    g32, c32 = compare(Qg, Q32)
+    g64, c64 = compare(Qg, Q64)
+    r64, rc64 = compare(Q32, Q64)
+    fmt = lambda v: ["%.2e" % x for x in v]
+    print(f"C2 {its} iterations, gpucmp / per cell rho,E: GPU vs oracle f32 {fmt(g32)} {fmt(c32)}; "
+          f"GPU vs FP64 {fmt(g64)} {fmt(c64)}; oracle f32 vs FP64 {fmt(r64)} {fmt(rc64)}")
+    for a, b in zip(g64 + c64, r64 + rc64):
+        assert a <= 1.5 * b, (g64, c64, r64, rc64)
+    r = ac.ref
+    fg = s.forces(3.0, 0.6, r["S"], r["xcg"], 0.0, r["c"])
+    f64 = o64.forces(3.0, 0.6, r["S"], r["xcg"], 0.0, r["c"])
+    print(f"C_L / C_D: GPU {fg['CL']:.7f} / {fg['CD']:.7f}, FP64 {f64['CL']:.7f} / {f64['CD']:.7f}")
+    assert sig4(fg["CL"]) == sig4(f64["CL"]) and sig4(fg["CD"]) == sig4(f64["CD"])
     s.dispose()
 
 
@@ -91,10 +128,18 @@ def test_c5_airliner_120m_spot_parity(aero, ref):
         assert m.sum() > 0, k
         for c in range(5):
             assert np.all(Qg[c][m] == np.float32(fix[k - 3][c])), (k, c)
-    del tt, geo
-    # forces and Trefftz drag from one state on both sides (FP64 reductions)
-    s.write(Qo.astype(np.float32))
-    del Qg
+    del tt, geo, Qg
+    # forces and Trefftz drag from one state on both sides (FP64 reductions).  Two iterations
+    # leave the Trefftz plane in the free stream (an integral of rounding noise), so the state
+    # gets a seeded cross-flow perturbation first, the same float32 values on both sides.
+    Q = Qo.astype(np.float32)
+    del Qo
+    rng = np.random.default_rng(5)
+    for c in (1, 2, 3):
+        Q[c] += (0.02 * rng.standard_normal(Q.shape[1], dtype=np.float32)) * Q[0]
+    s.write(Q)
+    o.write(Q.astype(np.float64))
+    del Q
     r = ac.ref
     fg = s.forces(2.5, 0.78, r["S"], r["xcg"], 0.0, r["c"])
     fo = o.forces(2.5, 0.78, r["S"], r["xcg"], 0.0, r["c"])

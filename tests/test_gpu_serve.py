@@ -25,7 +25,7 @@ def test_results_in_the_mix_equal_results_alone(aero, fix):
     sv.close()
     assert st["completed"] == len(reqs) and st["rounds"] < sum(m["iterations"] for m in mixed) / KW["chunk"]
     for r, m in zip(reqs, mixed):
-        alone = serve.solve_plain(r, kz=16, chunks=1, **KW)  # the served cases' configuration
+        alone = serve.solve_plain(r, kernel=serve.SERVED_KERNEL, kz=16, chunks=1, **KW)  # the served configuration
         assert m["status"] == 0 and m["iterations"] == alone["iterations"]
         for k in ("CL", "CD", "Cm", "CDi"):
             assert abs(m[k] - alone[k]) <= 1e-12 * max(1.0, abs(alone[k])), (r, k, m[k], alone[k])

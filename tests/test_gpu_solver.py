@@ -5,9 +5,12 @@ float64 like the reference's JavaScript CPU path; both store float32.  After the
 case's 200 iterations:
   * per-cell relative difference of rho and E (the variables that never cross zero) <= 3e-6;
   * the reference's GPU/CPU metric max|gpu - cpu| / max|cpu| (tools/gpucmp.mjs:19-21) <= 3e-6
-    for rho, rho*u and E, and <= 4e-6 for the transverse momenta rho*v, rho*w, whose largest
-    values are 4-7 times smaller than rho*u's (the oracle's own float32 run differs from its
-    float64 run by 1.8e-6 on rho*v under the same metric);
+    for all five variables with the default stage kernel (4; measured 2.8e-6 at most, on
+    rho*v).  The two cross-check kernels (0, one thread per cell, and 2, the single-cell TMA
+    tile) are held to 3e-6 on rho, rho*u and E and 4e-6 on the transverse momenta rho*v,
+    rho*w, whose largest values are 4-7 times smaller than rho*u's (measured 3.8e-6 and
+    3.2e-6 on rho*v; the oracle's own float32 run differs from its float64 run by 1.8e-6 on
+    rho*v under the same metric);
   * C_L and C_D agree to 4 significant digits and reproduce README.md:98.
 Post-processing reductions are FP64 on both sides: 1e-9 relative.
 """
@@ -24,7 +27,7 @@ TOL_CELL = 3e-6                               # per-cell relative, rho and E
 TOL_GPUCMP = [3e-6, 3e-6, 4e-6, 4e-6, 3e-6]  # max|d| / max|cpu| per variable
 
 
-def gpu_case(aero, sh, cells, delta, M=0.6, alpha=3.0, kernel=1, fix=None):
+def gpu_case(aero, sh, cells, delta, M=0.6, alpha=3.0, kernel=4, fix=None):
     g = aero.cfd_grid(sh, cells)
     s = aero.CfdGPU(g, shape=sh, delta=delta)
     s.set_kernel(kernel)
@@ -39,7 +42,7 @@ def sig4(x):
     return float(f"{x:.4g}")
 
 
-@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("kernel", [0, 2, 4])
 def test_readme_case_matches_oracle_and_pin(aero, ref, kernel):
     ac, sh, og, ogeo, o = oracle_case(aero, ref, "fighter", 30000, 3.0)
     g, s = gpu_case(aero, sh, 30000, 3.0, kernel=kernel)
@@ -47,9 +50,12 @@ def test_readme_case_matches_oracle_and_pin(aero, ref, kernel):
     s.step(200)
     Qo, Qg = o.read(), s.read_array()
     errs = [rel_max_diff(Qg[c], Qo[c]) for c in range(5)]
-    assert all(e <= t for e, t in zip(errs, TOL_GPUCMP)), errs
-    for c in (0, 4):
-        assert float(np.max(np.abs(Qg[c] - Qo[c]) / np.abs(Qo[c]))) <= TOL_CELL, c
+    cell = [float(np.max(np.abs(Qg[c] - Qo[c]) / np.abs(Qo[c]))) for c in (0, 4)]
+    print(f"README case, kernel {kernel}: gpucmp {['%.2e' % e for e in errs]}, per cell rho/E "
+          f"{['%.2e' % c for c in cell]}")
+    tol = [TOL_CELL] * 5 if kernel == 4 else TOL_GPUCMP  # the default kernel meets 3e-6 on all five
+    assert all(e <= t for e, t in zip(errs, tol)), errs
+    assert all(c <= TOL_CELL for c in cell), cell
     r = ac.ref
     fg = s.forces(3.0, 0.6, r["S"], r["xcg"], 0.0, r["c"])
     fo = o.forces(3.0, 0.6, r["S"], r["xcg"], 0.0, r["c"])
@@ -177,7 +183,7 @@ def test_read_dt_is_the_last_iterations_local_time_step(aero):
     assert float(np.max(np.abs(dt[fluid] - ref[fluid]) / ref[fluid])) < 2e-6
 
 
-@pytest.mark.parametrize("kernel", [1, 2, 3, 4])
+@pytest.mark.parametrize("kernel", [2, 4])
 def test_kernels_agree(aero, kernel):
     """The tiled kernels against the per-cell one (same float32 arithmetic, other summation order)."""
     sh = aero.shape_of(aero.build_aircraft("airliner"))
@@ -191,7 +197,7 @@ def test_kernels_agree(aero, kernel):
 
 @pytest.mark.parametrize("seed,dims,order", [(0, (9, 7, 6), 2), (1, (33, 9, 20), 2), (2, (40, 17, 3), 1),
                                              (3, (5, 2, 35), 2), (4, (64, 12, 18), 2)])
-@pytest.mark.parametrize("kernel", [0, 1, 2, 3, 4])
+@pytest.mark.parametrize("kernel", [0, 2, 4])
 def test_random_boxes_per_cell(aero, ref, seed, dims, order, kernel):
     """Random cut cells, solids, fixed cells and baffles; every cell after 1 and 15 iterations."""
     rng = np.random.default_rng(seed)

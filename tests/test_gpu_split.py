@@ -70,7 +70,7 @@ def test_pushing_slabs_refuse_unordered_use(aero):
     with pytest.raises(aero.AeroError):
         aero.Batch([s0, s1])                        # slab solvers are not batched
     with pytest.raises(aero.AeroError):
-        s0.set_kernel(1, 16) or s0.stage(1)         # the march kernel cannot push
+        s0.set_kernel(1, 16)                        # retired stage kernel numbers are refused
     sc.dispose()
 
 
