@@ -111,11 +111,12 @@ void make_room(a3d_server* sv, size_t need) {
 }
 
 // The coarse case of a sequenced request: cells / sequence, same shape and delta, free stream.
-// The per-case stage configuration of served cases: the TMA tile with the configured z run and
-// one launch per stage.  The cases already run concurrently in the server's batch, so the z
-// chunks that speed up a lone case only add launches here.
+// The per-case stage configuration of served cases: the paired-cell tile with the configured z
+// run and one launch per stage.  The cases already run concurrently in the server's batch, so
+// the z chunks that speed up a lone case only add launches here.  (64 uneven cases advanced
+// together: 15.0 G cell-updates/s with this tile, 14.0 with the single-cell TMA tile.)
 int configure_case(a3d_server* sv, a3d_solver* s) {
-  int rc = a3d_solver_set_kernel(s, a3d::KERNEL_TMA, sv->cfg.kz);
+  int rc = a3d_solver_set_kernel(s, a3d::KERNEL_PAIR, sv->cfg.kz);
   if (rc == A3D_OK) rc = a3d_solver_set_chunks(s, 1);
   return rc;
 }

@@ -23,7 +23,7 @@ from .aircraft import build_aircraft, shape_of, trefftz_x
 from .cfd import CfdGPU, cfd_grid, freestream
 
 TYPES = ("airliner", "interceptor", "fighter")
-SERVED_KERNEL = 2  # the stage kernel the server configures its cases with (server.cpp configure_case)
+SERVED_KERNEL = 4  # the stage kernel the server configures its cases with (server.cpp configure_case)
 _AIRCRAFT = {}
 
 

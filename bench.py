@@ -41,12 +41,14 @@ KERNEL_NAMES = {0: "k_stage_cell", 2: "k_stage_tma", 4: "k_stage_pair"}
 
 
 def measured_traffic(kernel, cells):
-    """DRAM bytes per RK stage from the committed ncu summary (profiles/), scaled to `cells`.
+    """DRAM bytes per RK stage from the committed ncu summary of the kernel (profiles/), scaled to
+    `cells`.
 
-    The summary lists, per kernel, `traffic <kernel> <bytes per cell-stage>` measured as
-    dram__bytes_read.sum + dram__bytes_write.sum on the 4.13M-cell fighter, summed over the four
-    z-chunk launches of a stage (mean of stage 1 and stage 2)."""
-    path = os.path.join(ROOT, "profiles", "stage_kernels_fighter4M.md")
+    The summary holds a line `traffic <kernel> <bytes per cell-stage>`: dram__bytes_read.sum +
+    dram__bytes_write.sum over whole stages of the 4.13M-cell fighter (k_stage_pair: a range
+    capture of 20 iterations, write-backs included; k_stage_tma: per-launch captures)."""
+    short = kernel[len("k_stage_"):] if kernel.startswith("k_stage_") else kernel
+    path = os.path.join(ROOT, "profiles", f"stage_{short}_fighter4M.md")
     if not os.path.exists(path):
         return None
     for line in open(path):
@@ -92,6 +94,10 @@ def parse():
     p.add_argument("--no-serve", action="store_true")
     p.add_argument("--no-c5", action="store_true", help="skip the 120M-cell airliner leg")
     p.add_argument("--c5-iters", type=int, default=200)
+    p.add_argument("--profile-range", action="store_true",
+                   help="bracket the device-resident timed steps by cudaProfilerStart/Stop, so that a profiler "
+                        "in range mode counts their DRAM traffic as a whole (write-backs of earlier launches "
+                        "included)")
     return p.parse_args()
 
 
@@ -268,7 +274,7 @@ def bench_batched(aero, args, ws, rank, local):
     for r in reqs:
         c = aero.Case(aircraft_type=r["type"], cells=r["cells"], M=r["M"], alpha=r["alpha"], delta=r["delta"],
                       device=local, fixed=r["fix"])
-        c.solver.set_kernel(4, 0)  # plain loop: each lone case's fastest kernel, z run and z chunks
+        c.solver.set_kernel(args.kernel, 0)  # plain loop: each lone case's automatic z run and z chunks
         cases.append(c)
     cells = sum(c.g.N for c in cases)
     it = args.batch_iters
@@ -283,8 +289,9 @@ def bench_batched(aero, args, ws, rank, local):
     torch.cuda.synchronize()
     t_plain = max_over_ranks(time.perf_counter() - t0, ws)
     # batched: the cases run concurrently, so each keeps one launch per stage and the 16-plane run
+    # (the persistent kernel's z run is the tuner's choice)
     for c in cases:
-        c.solver.set_kernel(2, 16)
+        c.solver.set_kernel(args.kernel, 16)
         c.solver.set_chunks(1)
     b = aero.Batch([c.solver for c in cases])
     tuned = b.tune(4)
@@ -483,11 +490,15 @@ def main():
     torch.cuda.synchronize()
     clk.start()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if args.profile_range:
+        torch.cuda.profiler.start()
     e0.record(stream)
     for _ in range(args.steps):
         f = solve()
     e1.record(stream)
     e1.synchronize()
+    if args.profile_range:
+        torch.cuda.profiler.stop()
     clocks = clk.stop()
     ms = e0.elapsed_time(e1) / args.steps
     ms = max_over_ranks(ms, ws)
