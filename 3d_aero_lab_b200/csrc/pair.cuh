@@ -27,8 +27,15 @@ __constant__ f2 kPkG = {kG, kG}, kPkIgm = {1.0f / kGm, 1.0f / kGm}, kPkHalf = {0
 __device__ __forceinline__ f2 add(f2 a, f2 b) { return __fadd2_rn(a, b); }
 __device__ __forceinline__ f2 mul(f2 a, f2 b) { return __fmul2_rn(a, b); }
 __device__ __forceinline__ f2 fma(f2 a, f2 b, f2 c) { return __ffma2_rn(a, b, c); }
-// a - b as (-1) b + a: one packed FMA, exact in the product, so the same value as a subtraction
-__device__ __forceinline__ f2 sub(f2 a, f2 b) { return __ffma2_rn(b, make_float2(-1.f, -1.f), a); }
+// a - b: the packed subtraction (FADD2 with a negated operand), no constant operand to stage
+__device__ __forceinline__ f2 sub(f2 a, f2 b) {
+  f2 r;
+  asm("{\n .reg .b64 ra, rb, rd;\n mov.b64 ra, {%2, %3};\n mov.b64 rb, {%4, %5};\n"
+      " sub.rn.f32x2 rd, ra, rb;\n mov.b64 {%0, %1}, rd;\n}"
+      : "=f"(r.x), "=f"(r.y)
+      : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
+  return r;
+}
 
 __device__ __forceinline__ f2 mn(f2 a, f2 b) { return make_float2(fminf(a.x, b.x), fminf(a.y, b.y)); }
 __device__ __forceinline__ f2 mx(f2 a, f2 b) { return make_float2(fmaxf(a.x, b.x), fmaxf(a.y, b.y)); }

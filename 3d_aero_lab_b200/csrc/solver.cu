@@ -254,6 +254,8 @@ int solver_finish_setup(a3d_solver* s) {
   const long N = s->N;
   s->NXp = (int)round_up(s->grid.NX, 16);
   s->Np = round_up((long)s->NXp * s->grid.NY * s->grid.NZ, 64);
+  // the tiled stage kernels index cells and padded cells of one component in 32-bit integers
+  A3D_ARG(s->Np < (1L << 31), "grid too large: more than 2^31 padded cells per component");
   A3D_CUDA(cudaMalloc(&s->state, 3 * 5 * s->Np * sizeof(float)));
   for (int b = 0; b < 3; b++) s->buf[b] = s->state + (long)b * 5 * s->Np;
   A3D_CUDA(cudaMemsetAsync(s->state, 0, 3 * 5 * s->Np * sizeof(float), s->st));

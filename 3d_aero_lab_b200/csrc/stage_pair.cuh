@@ -146,7 +146,7 @@ __device__ __forceinline__ uint32_t slot_pair(const StageArgs& a, const Slot& s,
 // the left and of this pair.  The slopes of cells x0-1, x0, x0+1 are each formed once.
 // G: aperture-weighted fluxes (mass, x-, y-, z-momentum, energy); returns the apertures.
 __device__ __forceinline__ f2 xfaces(const StageArgs& a, const PairSmem& S, int y, int p, const f2 c[5], uint32_t cl,
-                                     uint32_t cc, int x0, int jj, int k, uint32_t okm, f2 G[5]) {
+                                     uint32_t cc, int q, uint32_t okm, f2 G[5]) {
   const float h1 = half_if((cl >> 8) & okm, C_OKX), h2 = half_if(cc & okm, C_OKX);
   const float h3 = half_if((cc >> 8) & okm, C_OKX);
   f2 Ls[5], Rs[5];
@@ -160,12 +160,10 @@ __device__ __forceinline__ f2 xfaces(const StageArgs& a, const PairSmem& S, int 
     Rs[v] = make_float2(fmaf(-h2, s2, p2), fmaf(-h3, s3, p3));
   }
   // face x0-1/2 is cell x0-1's +x face, face x0+1/2 cell x0's (src/air_cfd.js:211, 223-224)
+  // q: geometry index of cell x0; a cell outside the domain carries a ghost code, never C_IRR
   f2 A = f2s(1.f);
-  if (jj < a.NY) {
-    const long q = ((long)k * a.NY + jj) * a.NX + x0;
-    if (x0 - 1 >= 0 && x0 - 1 < a.NX && ((cl >> 8) & C_IRR)) A.x = __ldg(a.ap0 + q - 1);
-    if (x0 < a.NX && (cc & C_IRR)) A.y = __ldg(a.ap0 + q);
-  }
+  if ((cl >> 8) & C_IRR) A.x = __ldg(a.ap0 + q - 1);
+  if (cc & C_IRR) A.y = __ldg(a.ap0 + q);
   // a closed face (A = 0) contributes A * F = 0: the flux of its finite states is formed
   // anyway, without a branch (src/air_cfd.js:223-224 skips it)
   f2 F[5];
@@ -178,7 +176,7 @@ __device__ __forceinline__ f2 xfaces(const StageArgs& a, const PairSmem& S, int 
 // y faces j-1/2 of the two cells (x0, x0+1) at plane-array pair p, row y (cell row jj, plane
 // k).  c: their primitives; cb, cc: codes of the pair in row y-1 and of this pair.
 __device__ __forceinline__ f2 yfaces(const StageArgs& a, const PairSmem& S, int y, int p, const f2 c[5], uint32_t cb,
-                                     uint32_t cc, int x0, int jj, int k, uint32_t okm, f2 G[5]) {
+                                     uint32_t cc, int qb, uint32_t okm, f2 G[5]) {
   const f2 hL = make_float2(half_if(cb & okm, C_OKY), half_if(cb & okm, C_OKY << 8));
   const f2 hR = make_float2(-half_if(cc & okm, C_OKY), -half_if(cc & okm, C_OKY << 8));
   f2 Ls[5], Rs[5];
@@ -192,12 +190,10 @@ __device__ __forceinline__ f2 yfaces(const StageArgs& a, const PairSmem& S, int 
     Rs[v] = fma(hR, sR, c[v]);
   }
   // face j-1/2 is cell (x, j-1)'s +y face; below y = 0 lies the symmetry mirror (open)
+  // qb: geometry index of cell (x0, jj-1); ghost and mirror codes never carry C_IRR
   f2 A = f2s(1.f);
-  if (jj - 1 >= 0 && jj - 1 < a.NY) {
-    const long q = ((long)k * a.NY + (jj - 1)) * a.NX + x0;
-    if (x0 < a.NX && (cb & C_IRR)) A.x = __ldg(a.ap1 + q);
-    if (x0 + 1 < a.NX && (cb & (C_IRR << 8))) A.y = __ldg(a.ap1 + q + 1);
-  }
+  if (cb & C_IRR) A.x = __ldg(a.ap1 + qb);
+  if (cb & (C_IRR << 8)) A.y = __ldg(a.ap1 + qb + 1);
   f2 F[5];  // closed faces: A * F = 0, no branch
   hllc2(PP{Ls[0], Ls[2], Ls[1], Ls[3], Ls[4]}, PP{Rs[0], Rs[2], Rs[1], Rs[3], Rs[4]}, F);
   G[0] = mul(A, F[0]); G[1] = mul(A, F[2]); G[2] = mul(A, F[1]); G[3] = mul(A, F[3]); G[4] = mul(A, F[4]);
@@ -209,8 +205,8 @@ __device__ __forceinline__ f2 yfaces(const StageArgs& a, const PairSmem& S, int 
 // c's slope gives this face's right state and, in Lc, the left state of the face above: each
 // z slope is formed once.  qb: geometry index of b's first cell.
 __device__ __forceinline__ f2 zfaces(const StageArgs& a, const f2 Lb[5], const f2 Pb[5], const f2 Pc[5],
-                                     const f2 Pe[5], uint32_t cb, uint32_t cc, bool b_in_domain, long qb, bool in0,
-                                     bool in1, uint32_t okm, f2 G[5], f2 Lc[5]) {
+                                     const f2 Pe[5], uint32_t cb, uint32_t cc, int qb, uint32_t okm, f2 G[5],
+                                     f2 Lc[5]) {
   const f2 h = make_float2(half_if(cc & okm, C_OKZ), half_if(cc & okm, C_OKZ << 8));
   const f2 hn = make_float2(-h.x, -h.y);
   f2 Rc[5];
@@ -221,11 +217,10 @@ __device__ __forceinline__ f2 zfaces(const StageArgs& a, const f2 Lb[5], const f
     Rc[v] = fma(hn, s, Pc[v]);
     Lc[v] = fma(h, s, Pc[v]);
   }
+  // cells outside the domain carry ghost codes, never C_IRR
   f2 A = f2s(1.f);
-  if (b_in_domain) {
-    if (in0 && (cb & C_IRR)) A.x = __ldg(a.ap2 + qb);
-    if (in1 && (cb & (C_IRR << 8))) A.y = __ldg(a.ap2 + qb + 1);
-  }
+  if (cb & C_IRR) A.x = __ldg(a.ap2 + qb);
+  if (cb & (C_IRR << 8)) A.y = __ldg(a.ap2 + qb + 1);
   f2 F[5];  // closed faces: A * F = 0, no branch
   hllc2(PP{Lb[0], Lb[3], Lb[1], Lb[2], Lb[4]}, PP{Rc[0], Rc[3], Rc[1], Rc[2], Rc[4]}, F);
   G[0] = mul(A, F[0]); G[1] = mul(A, F[2]); G[2] = mul(A, F[3]); G[3] = mul(A, F[1]); G[4] = mul(A, F[4]);
@@ -235,7 +230,7 @@ __device__ __forceinline__ f2 zfaces(const StageArgs& a, const f2 Lb[5], const f
 // Baffle transpiration of one cell (src/air_cfd.js:226-233): w = u dz/dx through the +z face
 // (slope sUp = ap3 of the cell) and the -z face (sDn = ap3 of the cell below), with the cell's
 // own state; Am, Ap: the cell's -z and +z apertures.
-__device__ __forceinline__ void baffle(const StageArgs& a, long q, int k, long NXY, float r, float u, float v, float w,
+__device__ __forceinline__ void baffle(const StageArgs& a, int q, int k, int NXY, float r, float u, float v, float w,
                                        float pC, float Am, float Ap, float rz, float R[5]) {
   const float sUp = __ldg(a.ap3 + q), sDn = k > 0 ? __ldg(a.ap3 + q - NXY) : 0.f;
   if (sUp != 0.f || sDn != 0.f) {
@@ -292,7 +287,9 @@ __device__ __forceinline__ bool stage_tile(PairSmem& S, const CUtensorMap* tmQ, 
   // the halo (and so every cell the tile reads) inside the domain in x and y; own cells inside
   const bool tile_in = i0 >= 2 && i0 + TX + 2 <= a.NX && j0 >= 2 && j0 + TY + 2 <= a.NY;
   const bool own_in = i0 + TX <= a.NX && j0 + TY <= a.NY;
-  const long NXY = (long)a.NX * a.NY, Np = a.Np;
+  const int NXY = a.NX * a.NY, PL = a.NY * a.NXp;  // plane strides of the geometry and state arrays
+  const int q0 = j * a.NX + x0, qp0 = j * a.NXp + x0;  // this pair's indices in plane 0
+  const long Np = a.Np;
   const uint32_t okm = a.order2 ? 0xFFFFu : 0u;  // slope flags count only at second order
   const f2 rx = make_float2(in0 ? a.rXd[x0] : 0.f, in1 ? a.rXd[x0 + 1] : 0.f);
   const f2 ry = f2s(jin ? a.rYd[j] : 0.f);
@@ -341,8 +338,7 @@ __device__ __forceinline__ bool stage_tile(PairSmem& S, const CUtensorMap* tmQ, 
       const f2 d1 = sub(Wm[v], Wa[v]), d2 = sub(W0[v], Wm[v]);
       Lm[v] = fma(hm, make_float2(minmod(d1.x, d2.x), minmod(d1.y, d2.y)), Wm[v]);
     }
-    Az = zfaces(a, Lm, Wm, W0, W1, cm, c0, k0 - 1 >= 0, ((long)(k0 - 1) * a.NY + j) * a.NX + x0, in0, in1, okm, Gz,
-                Lz);
+    Az = zfaces(a, Lm, Wm, W0, W1, cm, c0, (k0 - 1) * NXY + q0, okm, Gz, Lz);
   }
   if (!ok) S.abort = 1;
   __syncthreads();  // slots of planes k0-2 and k0-1 are free again
@@ -357,6 +353,8 @@ __device__ __forceinline__ bool stage_tile(PairSmem& S, const CUtensorMap* tmQ, 
 
   for (int k = k0; k < k1; k++) {
     const int sk = slot_of(k, k0), sk2 = slot_of(k + 2, k0);
+    const int q = k * NXY + q0;    // geometry index of the pair's first cell
+    const int qp = k * PL + qp0;   // padded state index of the pair
     // ---- [A] plane k to shared memory ----
 #pragma unroll
     for (int v = 0; v < 5; v++) S.P[v][hy][pp] = W0[v];
@@ -381,14 +379,14 @@ __device__ __forceinline__ bool stage_tile(PairSmem& S, const CUtensorMap* tmQ, 
     // ---- [B] x and y face fluxes ----
     {
       f2 G[5];
-      const f2 A = xfaces(a, S, hy, pp, W0, S.C[hy][pp - 1], c0, x0, j, k, okm, G);
+      const f2 A = xfaces(a, S, hy, pp, W0, S.C[hy][pp - 1], c0, q, okm, G);
 #pragma unroll
       for (int v = 0; v < 5; v++) S.Fx[v][ty][tx2] = G[v];
       S.Ax[ty][tx2] = A;
     }
     {
       f2 G[5];
-      const f2 A = yfaces(a, S, hy, pp, W0, S.C[hy - 1][pp], c0, x0, j, k, okm, G);
+      const f2 A = yfaces(a, S, hy, pp, W0, S.C[hy - 1][pp], c0, q - a.NX, okm, G);
 #pragma unroll
       for (int v = 0; v < 5; v++) S.Fy[v][ty][tx2] = G[v];
       S.Ay[ty][tx2] = A;
@@ -398,7 +396,8 @@ __device__ __forceinline__ bool stage_tile(PairSmem& S, const CUtensorMap* tmQ, 
       f2 c[5], G[5];
 #pragma unroll
       for (int v = 0; v < 5; v++) c[v] = S.P[v][TY + 2][e + 1];
-      const f2 A = yfaces(a, S, TY + 2, e + 1, c, S.C[TY + 1][e + 1], S.C[TY + 2][e + 1], i0 + 2 * e, j0 + TY, k, okm, G);
+      const f2 A = yfaces(a, S, TY + 2, e + 1, c, S.C[TY + 1][e + 1], S.C[TY + 2][e + 1],
+                          k * NXY + (j0 + TY - 1) * a.NX + i0 + 2 * e, okm, G);
 #pragma unroll
       for (int v = 0; v < 5; v++) S.Fy[v][TY][e] = G[v];
       S.Ay[TY][e] = A;
@@ -407,14 +406,13 @@ __device__ __forceinline__ bool stage_tile(PairSmem& S, const CUtensorMap* tmQ, 
       f2 c[5], G[5];
 #pragma unroll
       for (int v = 0; v < 5; v++) c[v] = S.P[v][r + 2][TX / 2 + 1];
-      const f2 A = xfaces(a, S, r + 2, TX / 2 + 1, c, S.C[r + 2][TX / 2], S.C[r + 2][TX / 2 + 1], i0 + TX, j0 + r, k,
-                          okm, G);
+      const f2 A = xfaces(a, S, r + 2, TX / 2 + 1, c, S.C[r + 2][TX / 2], S.C[r + 2][TX / 2 + 1],
+                          k * NXY + (j0 + r) * a.NX + i0 + TX, okm, G);
 #pragma unroll
       for (int v = 0; v < 5; v++) S.Fx[v][r][TX / 2] = G[v];
       S.Ax[r][TX / 2] = A;
     }
     f2 bq[5];
-    const long qp = ((long)k * a.NY + j) * a.NXp + x0;  // padded state index of the pair
     if (STAGE2 && in0) {
 #pragma unroll
       for (int c = 0; c < 5; c++) bq[c] = __ldg(reinterpret_cast<const float2*>(Bp + c * Np + qp));
@@ -426,8 +424,7 @@ __device__ __forceinline__ bool stage_tile(PairSmem& S, const CUtensorMap* tmQ, 
     if (!ok) S.abort = 1;
     f2 W2[5], Gn[5], Ln[5];
     const uint32_t c2 = own(k + 2, W2);
-    const long q = ((long)k * a.NY + j) * a.NX + x0;  // geometry index of the pair's first cell
-    const f2 An = zfaces(a, Lz, W0, W1, W2, c0, c1, true, q, in0, in1, okm, Gn, Ln);
+    const f2 An = zfaces(a, Lz, W0, W1, W2, c0, c1, q, okm, Gn, Ln);
     __syncthreads();
     if (S.abort) { first_pending = k + 2; break; }  // the wait for plane k+2 ran out
     // ---- [C] residual and RK update ----

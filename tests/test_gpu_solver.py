@@ -71,7 +71,7 @@ def test_engine_field_fixed_states_match_oracle(aero, ref, typ, cells, h, M, alp
     ac = aero.build_aircraft(typ)
     fix = aero.fix_states(ac, h, M, alpha, 1.0, ab)[1]
     _, sh, og, ogeo, o = oracle_case(aero, ref, typ, cells, 0.0, M=M, alpha=alpha, fix=fix)
-    g, s = gpu_case(aero, sh, cells, 0.0, M=M, alpha=alpha, kernel=2, fix=fix)
+    g, s = gpu_case(aero, sh, cells, 0.0, M=M, alpha=alpha, kernel=4, fix=fix)
     t = np.asarray(ogeo.t)
     assert (t == 5).sum() > 0
     o.step(200)
@@ -79,7 +79,8 @@ def test_engine_field_fixed_states_match_oracle(aero, ref, typ, cells, h, M, alp
     Qo, Qg = o.read(), s.read_array()
     assert np.all(np.isfinite(Qg))
     errs = [rel_max_diff(Qg[c], Qo[c]) for c in range(5)]
-    assert all(e <= tl for e, tl in zip(errs, TOL_GPUCMP)), errs
+    print(f"{typ} field-model fixed states: gpucmp {['%.2e' % e for e in errs]}")
+    assert all(e <= TOL_CELL for e in errs), errs
     for k in (3, 4, 5):  # fixed cells keep their state
         for c in range(5):
             assert np.all(Qg[c][t == k] == np.float32(fix[k - 3][c])), (k, c)
@@ -93,18 +94,20 @@ def test_engine_field_fixed_states_match_oracle(aero, ref, typ, cells, h, M, alp
                                                      ("airliner", 40000, 0.3, -2.0, 5.0)])
 def test_batch_distribution_corners_match_oracle(aero, ref, typ, cells, M, alpha, delta):
     """Corners of the batched/served case distribution (M 0.3-0.85, alpha -2..8, delta -5..5) on
-    the other two aircraft: the default kernel against the oracle, same tolerances as the README
-    case."""
+    the other two aircraft: the default kernel against the oracle.  Per cell 3e-6 for rho and E;
+    on the reference's metric 3e-6 for rho, rho*u, E and 4e-6 for the transverse momenta (measured
+    3.1e-6 on rho*v at the airliner corner, M0.3 alpha -2 delta 5)."""
     ac, sh, og, ogeo, o = oracle_case(aero, ref, typ, cells, delta, M=M, alpha=alpha)
-    g, s = gpu_case(aero, sh, cells, delta, M=M, alpha=alpha, kernel=2)
+    g, s = gpu_case(aero, sh, cells, delta, M=M, alpha=alpha, kernel=4)
     o.step(200)
     s.step(200)
     Qo, Qg = o.read(), s.read_array()
     assert np.all(np.isfinite(Qg))
     errs = [rel_max_diff(Qg[c], Qo[c]) for c in range(5)]
+    cell = [float(np.max(np.abs(Qg[c] - Qo[c]) / np.abs(Qo[c]))) for c in (0, 4)]
+    print(f"{typ} corner: gpucmp {['%.2e' % e for e in errs]}, per cell rho/E {['%.2e' % c for c in cell]}")
     assert all(e <= t for e, t in zip(errs, TOL_GPUCMP)), errs
-    for c in (0, 4):
-        assert float(np.max(np.abs(Qg[c] - Qo[c]) / np.abs(Qo[c]))) <= TOL_CELL, c
+    assert all(c <= TOL_CELL for c in cell), cell
     r = ac.ref
     fg = s.forces(alpha, M, r["S"], r["xcg"], 0.0, r["c"])
     fo = o.forces(alpha, M, r["S"], r["xcg"], 0.0, r["c"])
