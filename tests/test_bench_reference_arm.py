@@ -46,3 +46,14 @@ def test_reference_arm_under_torchrun_prints_on_rank_zero_only():
     assert r.returncode == 0, r.stderr[-2000:]
     lines = json_lines(r.stdout)
     assert len(lines) == 1 and lines[0]["impl"] == "reference" and lines[0]["n_gpus"] == 2
+
+
+def test_roofline_traffic_comes_from_the_kernels_profile_summary():
+    """roofline.traffic is the committed range capture of the default kernel (DRAM bytes per cell
+    and stage over whole stages) times the cells; a kernel without a summary reports none."""
+    import bench
+    n = 4131324
+    assert bench.measured_traffic("k_stage_pair", n) == 52.6 * n
+    assert bench.measured_traffic("k_stage_tma", n) == 35.8 * n
+    assert bench.measured_traffic("k_stage_cell", n) is None
+    assert bench.KERNEL_NAMES[4] == "k_stage_pair"
