@@ -1,9 +1,9 @@
 """One case on z slabs (split.py) against the same case unsplit, on one GPU.
 
 With the halo planes exchanged after each stage, a slab's own planes see the numbers of the
-unsplit solve.  The per-cell kernel and the z-marching TMA tile with slab boundaries aligned
-to its z runs give the same state bit for bit.  Unaligned, the TMA tile differs only where a
-z run starts elsewhere, within the 4e-6 of its prologue rounding.  The FP64 reductions sum
+unsplit solve.  The per-cell kernel and the z-marching TMA tiles (single-cell and paired) with
+slab boundaries aligned to their z runs give the same state bit for bit.  Unaligned, a tile
+differs only where a z run starts elsewhere, within the 4e-6 of its prologue rounding.  The FP64 reductions sum
 the same terms in another order.
 """
 import math
@@ -22,7 +22,7 @@ def full_case(aero, typ, cells, M, alpha, delta, kernel, fixed):
 
 @pytest.mark.parametrize("push", [True, False])
 @pytest.mark.parametrize("kernel,slabs,align,exact", [(0, 2, 1, True), (0, 3, 1, True), (2, 3, 16, True),
-                                                      (2, 2, 1, False)])
+                                                      (2, 2, 1, False), (4, 3, 16, True), (4, 2, 1, False)])
 def test_slabs_reproduce_the_unsplit_solve(aero, kernel, slabs, align, exact, push):
     """push: stage kernels store the neighbours' halo planes into their buffers; otherwise the
     halos are copied between the stages."""
